@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the LBM time step: D3Q19 256^3 square duct on B200.
+
+Workload (the configuration the headline metric is quoted on): D3Q19 TRT,
+tau = 0.9, Lambda = 3/16, 256 x 256 x 256 nodes, solid layers at y = 0, 255
+and z = 0, 255, periodic in x, Guo body force Fx = 1e-6, float32 storage.
+One bench "step" is one LBM time step over the whole lattice (one fused
+kernel launch). The lattice (2 x 1.27 GB) is ~20x the 126 MB L2, so every
+step streams from HBM; no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--variant pull|aa]
+                    [--storage float32|float16|bfloat16|float64] [--impl reference]
+
+Prints one JSON line (rank 0). ``value`` is whole-job MLUPS (all GPUs; each
+GPU runs its own replica of the duct: the step has no inter-GPU exchange in
+this build, so scaling is weak, replicas only). ``e2e`` is MLUPS through the
+public API with host buffers: per e2e step, ``initialize`` from pinned host
+rho/u (float64), ``run`` of a chunk of time steps, ``macroscopic`` back to the
+host. ``roofline.achieved`` = MLUPS * 152 B (2 Q float32 per update, the
+reference's count, benchmarks/bench_mlups.py:9-10) over the kernel's CUDA-event
+time. ``cpu_baseline`` times the NumPy oracle (a restatement of the reference's
+CPU solver) on a bounded slab of the same duct on this host.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "D3Q19 256^3 MLUPS"
+BYTES = {"float32": 4, "float64": 8, "float16": 2, "bfloat16": 2}
+DTYPE_TAG = {"float32": "f32", "float64": "f64", "float16": "f16-store/f32", "bfloat16": "bf16-store/f32"}
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--variant", choices=("pull", "aa"), default="aa")
+    ap.add_argument("--storage", choices=tuple(BYTES), default="float32")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--e2e-iters", type=int, default=3)
+    ap.add_argument("--e2e-chunk", type=int, default=100)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def duct_params(lbm, n, nx=None, nz=None, storage="float32"):
+    nx = n if nx is None else nx
+    nz = n if nz is None else nz
+    solid = np.zeros((nz, n, nx), dtype=bool)
+    solid[:, [0, -1], :] = True
+    solid[[0, -1], :, :] = True
+    return lbm.SimulationParams(nx=nx, ny=n, nz=nz, tau=0.9, collision="trt", force=(1e-6, 0.0, 0.0),
+                                solid=solid, dtype=storage)
+
+
+# --------------------------------------------------------------------- CPU side
+def oracle_mlups(n: int, nz: int, steps: int, warmup: int, budget: float | None = None):
+    """NumPy oracle on an n x n x nz slab of the duct: (MLUPS, steps timed, seconds)."""
+    import lbm_b200 as lbm
+    from oracle import OracleSolver
+
+    p = duct_params(lbm, n, nz=nz)
+    s = OracleSolver(p)
+    for _ in range(warmup):
+        s.step()
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps or (budget is not None and time.perf_counter() - t0 < budget and done < 10 * steps):
+        s.step()
+        done += 1
+        if budget is not None and time.perf_counter() - t0 >= budget and done >= 3:
+            break
+    dt = time.perf_counter() - t0
+    return n * n * nz * done / dt / 1e6, done, dt
+
+
+def run_reference(args, rank):
+    """Reference arm: the NumPy oracle port of the reference CPU solver, rank 0 only."""
+    if rank != 0:
+        return
+    n = args.n
+    # size the slab so that warm-up + K steps take about a minute
+    per_node = 1.0 / 1.4e6
+    nz = int(min(16, max(3, round(60.0 / (max(args.steps, 1) * n * n * per_node)))))
+    mlups, done, dt = oracle_mlups(n, nz, args.steps, args.warmup)
+    sample = f"{n}x{n}x{nz} slab of the duct (same walls, force, tau), {done} steps after {args.warmup} warm-up"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(mlups, 4), "unit": "MLUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / done, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "NumPy restatement of the reference ReferenceSolver (the reference is pure Python and is "
+                "not installed on the GPU host); NumPy element-wise work is single-threaded",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    n = args.n
+    return {
+        "workload": f"D3Q19 TRT square duct {n}x{n}x{n}, tau=0.9, Fx=1e-6, walls y/z, periodic x",
+        "variant": {"pull": "two-lattice fused pull", "aa": "in-place AA pair"}[args.variant],
+        "storage": args.storage, "nodes": n**3, "bytes_per_update": 2 * 19 * BYTES[args.storage],
+        "l2": "inputs larger than L2 (lattice %.2f GB vs 126 MB)" % (19 * n**3 * BYTES[args.storage] / 1e9),
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+# --------------------------------------------------------------------- GPU side
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid: str | None):
+        self.uuid = device_uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd.insert(1, f"--id={self.uuid}")
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        rows = [r.split(", ") for r in self.lines if r and r[0].isdigit()]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 4 + i and r[4 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][1]), "samples": len(rows),
+                "power_w_max": max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit()) if rows else None,
+                "reasons": reasons}
+
+
+def measured_peak():
+    try:
+        peaks = json.loads(PEAKS_FILE.read_text())
+        return float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, torch copy_ of 1 Gi bf16)"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(variant: str, storage: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists for this kernel/workload."""
+    path = ROOT / "profiles" / f"step_{variant}_d3q19_{storage}_duct.md"
+    if not path.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", path.read_text())
+    return float(m.group(1)) if m else None
+
+
+def copy_peak_gbs(torch, device, nbytes=512 * 2**20, repeats=20):
+    """Device copy bandwidth (read + write), as the reference measures it (bench_mlups.py:66-79)."""
+    src = torch.ones(nbytes // 4, dtype=torch.float32, device=device)
+    dst = torch.empty_like(src)
+    dst.copy_(src)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(repeats):
+        dst.copy_(src)
+    b.record()
+    b.synchronize()
+    del src, dst
+    return 2 * nbytes * repeats / (a.elapsed_time(b) / 1e3) / 1e9
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import lbm_b200 as lbm
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    n = args.n
+    nodes = n**3
+    params = duct_params(lbm, n, storage=args.storage)
+    backend = "cuda-aa" if args.variant == "aa" else "cuda-naive"
+    solver = lbm.make_solver(params, backend=backend)
+    steps = args.steps + (args.steps % solver.step_multiple)
+    warm = max(args.warmup, 3)
+    warm += warm % solver.step_multiple
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    stream = torch.cuda.current_stream()
+    solver._advance(warm)
+    barrier()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+    except Exception:  # noqa: BLE001
+        uuid = None
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(uuid) as clocks:
+        barrier()
+        start.record(stream)
+        solver._advance(steps)
+        stop.record(stream)
+        stop.synchronize()
+        barrier()
+    ms = start.elapsed_time(stop)
+    solver.time_step += warm + steps
+    solver._check_health()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    mlups = world * nodes * steps / (ms / 1e3) / 1e6
+    ms_step = ms / steps
+
+    # ---- end to end through the public API, host buffers in pinned memory
+    e2e = None
+    if not args.no_e2e:
+        shape = params.shape
+        rho_h = torch.ones(shape, dtype=torch.float64).pin_memory()
+        u_h = [torch.zeros(shape, dtype=torch.float64).pin_memory() for _ in range(3)]
+        chunk = args.e2e_chunk + args.e2e_chunk % solver.step_multiple
+        solver.initialize(rho_h, *u_h)
+        solver.run(chunk, check_every=chunk)
+        _ = solver.macroscopic()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_iters):
+            solver.initialize(rho_h, *u_h)
+            solver.run(chunk, check_every=chunk)
+            fields = solver.macroscopic()
+        barrier()
+        dt = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([dt], dtype=torch.float64, device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        h2d = 4 * nodes * 8
+        d2h = 4 * nodes * fields.rho.itemsize + 16
+        e2e = {"value": round(world * nodes * chunk * args.e2e_iters / dt / 1e6, 2), "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "step": f"initialize(pinned host rho,u f64) + run({chunk}) + macroscopic() to host",
+               "iters": args.e2e_iters}
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    bpu = 2 * 19 * BYTES[args.storage]
+    achieved = mlups / world * 1e6 * bpu / 1e9
+    traffic = profile_traffic(args.variant, args.storage)
+    copy_now = copy_peak_gbs(torch, device)
+    res = solver.kernel_resources()
+    line = {
+        "metric": METRIC, "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": world, "steps": steps,
+        "warmup": warm, "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": DTYPE_TAG[args.storage], "data": "synthetic (analytic duct set-up, fluid at rest)",
+        "config": workload_config(args),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_update": bpu, "copy_peak_in_run_gbs": round(copy_now, 1),
+                     "frac_of_copy_in_run": round(achieved / copy_now, 4)},
+        "gpu_launches": steps,
+        "kernel_resources": res,
+        "clocks": clocks.summary(),
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if not args.no_cpu_baseline and world == 1:
+        mlups_cpu, done, dt = oracle_mlups(n, 8, 3, 1, budget=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(mlups_cpu, 4), "unit": "MLUPS", "cores": 1, "kind": "port",
+                                "sample": f"{n}x{n}x8 slab of the duct, {done} steps in {dt:.1f} s (NumPy oracle, "
+                                          f"single-threaded element-wise; host has {os.cpu_count()} cores)"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

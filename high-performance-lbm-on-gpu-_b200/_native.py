@@ -1,0 +1,138 @@
+"""ctypes binding of ``liblbm_b200.so`` (declarations in ``include/lbm_b200.h``).
+
+The library is loaded lazily on first use and never silently replaced: if it
+is missing or cannot be loaded the caller gets ``NativeUnavailable``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "liblbm_b200.so"
+ABI_VERSION = 1
+
+LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH = 0, -1, -2, -3
+LBM_D2Q9, LBM_D3Q19 = 0, 1
+LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
+LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
+LAYOUT_PULL, LAYOUT_AA_ODD, LAYOUT_AA_EVEN = 0, 1, 2
+KIND_SOLID, KIND_SPECIAL, KIND_NEAR = 1, 2, 4
+
+STORAGE_CODE = {"float32": LBM_F32, "float64": LBM_F64, "float16": LBM_F16, "bfloat16": LBM_BF16}
+LATTICE_CODE = {"D2Q9": LBM_D2Q9, "D3Q19": LBM_D3Q19}
+
+vp = C.c_void_p
+i32, i64, u32 = C.c_int32, C.c_int64, C.c_uint32
+
+
+class NativeUnavailable(RuntimeError):
+    pass
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+class Grid(C.Structure):
+    _fields_ = [("lattice", i32), ("storage", i32), ("nx", i32), ("ny", i32), ("nz", i32), ("pitch", i32), ("qstride", i64)]
+
+
+class Physics(C.Structure):
+    _fields_ = [
+        ("omega_plus", C.c_double), ("omega_minus", C.c_double), ("force", C.c_double * 3),
+        ("wall_u", vp), ("force_field", vp),
+    ]
+
+
+class Special(C.Structure):
+    _fields_ = [
+        ("n_special", i32), ("node", vp), ("rule_mask", vp), ("rule_first", vp), ("force_slot", vp),
+        ("export_mask", vp), ("export_first", vp), ("n_rules", i32), ("n_terms", i32), ("term_start", vp),
+        ("rule_const", vp), ("term_dir", vp), ("term_node", vp), ("term_export", vp), ("term_coeff", vp),
+        ("local_force", vp), ("n_local", i32), ("n_export", i32), ("export_in", vp), ("export_out", vp),
+    ]
+
+
+class Launch(C.Structure):
+    _fields_ = [("tile_x", i32), ("tile_y", i32)]
+
+
+class Ibm(C.Structure):
+    _fields_ = [
+        ("n_nodes", i32), ("n_markers", i32), ("stencil_size", i32), ("node", vp), ("stencil", vp),
+        ("weight", vp), ("area", vp), ("inv_start", vp), ("inv_marker", vp), ("inv_weight", vp),
+        ("rho", vp), ("u_star", vp), ("marker_force", vp),
+    ]
+
+
+P = C.POINTER
+_SIGNATURES = {
+    "lbm_step_pull": [P(Grid), P(Physics), P(Special), P(Launch), vp, vp, vp, vp],
+    "lbm_step_aa": [P(Grid), P(Physics), P(Special), P(Launch), vp, vp, i32, vp],
+    "lbm_export_prime": [P(Grid), P(Special), vp, i32, vp, vp],
+    "lbm_classify": [P(Grid), vp, vp, i32, vp, vp],
+    "lbm_init_equilibrium": [P(Grid), P(Physics), vp, vp, i32, vp, vp],
+    "lbm_unpack": [P(Grid), vp, i32, vp, vp],
+    "lbm_pack": [P(Grid), vp, i32, vp, vp],
+    "lbm_macroscopic": [P(Grid), P(Physics), vp, vp, i32, vp, vp, i32, vp, vp, vp],
+    "lbm_health_reset": [vp, vp],
+    "lbm_health": [P(Grid), vp, vp, vp, vp],
+    "lbm_affine_gather": [i32, vp, vp, vp, vp, i64, i32, vp, vp],
+    "lbm_affine_reduce": [i32, vp, vp, vp, vp, vp, i64, i32, i32, vp, vp, vp, vp],
+    "lbm_ibm_moments": [P(Grid), P(Physics), P(Ibm), vp, i32, vp],
+    "lbm_ibm_iteration": [P(Grid), P(Ibm), i32, vp, vp, vp],
+    "lbm_ibm_body_force": [P(Grid), P(Ibm), i32, vp, vp],
+    "lbm_kernel_resources": [i32, i32, i32, vp],
+}
+EXPORTED = (*_SIGNATURES, "lbm_last_cuda_error", "lbm_abi_version")
+
+_lib = None
+
+
+def load(path: Path | None = None):
+    """Load the library once; raise ``NativeUnavailable`` if it cannot be loaded."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    target = Path(path) if path is not None else LIBRARY
+    if not target.exists():
+        raise NativeUnavailable(f"{target.name} is not built; run build() from __graft_entry__ or build.py")
+    try:
+        lib = C.CDLL(str(target))
+    except OSError as exc:
+        raise NativeUnavailable(f"cannot load {target}: {exc}") from exc
+    for name, args in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    lib.lbm_last_cuda_error.restype = C.c_char_p
+    lib.lbm_last_cuda_error.argtypes = []
+    lib.lbm_abi_version.restype = i32
+    lib.lbm_abi_version.argtypes = []
+    if lib.lbm_abi_version() != ABI_VERSION:
+        raise NativeUnavailable(f"{target.name} has ABI {lib.lbm_abi_version()}, expected {ABI_VERSION}")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int, what: str) -> None:
+    if status == LBM_OK:
+        return
+    lib = load()
+    if status == LBM_ERR_LAUNCH:
+        raise NativeError(f"{what}: CUDA launch failed ({lib.lbm_last_cuda_error().decode()})")
+    if status == LBM_ERR_UNSUPPORTED:
+        raise NativeError(f"{what}: unsupported configuration")
+    raise NativeError(f"{what}: invalid argument (status {status})")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args), name)
+
+
+def ptr(tensor) -> int | None:
+    """Device address of a torch tensor (None for None)."""
+    return None if tensor is None else tensor.data_ptr()

@@ -1,0 +1,125 @@
+// extern "C" entry points of the step (include/lbm_b200.h).
+#include "dispatch.cuh"
+
+using namespace lbm;
+
+static thread_local const char* g_last_error = "no error";
+
+static int record(int status)
+{
+    if (status == LBM_ERR_LAUNCH) g_last_error = cudaGetErrorString(cudaGetLastError());
+    return status;
+}
+
+static bool grid_valid(const lbm_grid_t* g)
+{
+    if (g == nullptr) return false;
+    if (g->lattice != LBM_D2Q9 && g->lattice != LBM_D3Q19) return false;
+    if (g->storage < LBM_F32 || g->storage > LBM_BF16) return false;
+    if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->pitch < g->nx) return false;
+    if (g->lattice == LBM_D2Q9 && g->nz != 1) return false;
+    return g->qstride == (int64_t)g->pitch * g->ny * g->nz;
+}
+
+static bool special_valid(const lbm_special_t* sp, bool aa)
+{
+    if (sp == nullptr) return true;
+    if (sp->n_special < 0 || sp->n_rules < 0 || sp->n_terms < 0 || sp->n_local < 0 || sp->n_export < 0) return false;
+    if (sp->n_special == 0) return true;
+    if (!sp->node || !sp->rule_mask || !sp->rule_first || !sp->force_slot) return false;
+    if (sp->n_rules > 0) {
+        if (!sp->term_start || !sp->rule_const || !sp->term_coeff) return false;
+        if (aa ? !sp->term_export : (!sp->term_dir || !sp->term_node)) return false;
+        if (aa && (!sp->export_in || sp->n_export <= 0)) return false;
+    }
+    if (aa && sp->n_export > 0 && (!sp->export_mask || !sp->export_first || !sp->export_out)) return false;
+    if (sp->n_local > 0 && !sp->local_force) return false;
+    return true;
+}
+
+static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
+                     const lbm_launch_t* launch, const uint8_t* kind, const void* src, void* dst, int& threads)
+{
+    const int tx = launch ? launch->tile_x : 32;
+    const int ty = launch ? launch->tile_y : 8;
+    if (tx <= 0 || ty <= 0 || tx % 32 != 0 || tx * ty > 256) return LBM_ERR_INVALID;
+    threads = tx * ty;
+    a.nx = g->nx;
+    a.ny = g->ny;
+    a.nz = g->nz;
+    a.pitch = g->pitch;
+    a.qstride = g->qstride;
+    a.tile_x = tx;
+    a.tile_y = ty;
+    a.tiles_x = (g->nx + tx - 1) / tx;
+    a.tiles_y = (g->ny + ty - 1) / ty;
+    a.bulk_blocks = (int64_t)a.tiles_x * a.tiles_y * g->nz;
+    a.wp = p->omega_plus;
+    a.wm = p->omega_minus;
+    a.fx = p->force[0];
+    a.fy = p->force[1];
+    a.fz = g->lattice == LBM_D3Q19 ? p->force[2] : 0.0;
+    a.kind = kind;
+    a.f_src = src;
+    a.f_dst = dst;
+    a.wall_u = p->wall_u;
+    a.force_field = p->force_field;
+    if (sp)
+        a.sp = *sp;
+    else
+        memset(&a.sp, 0, sizeof(a.sp));
+    return LBM_OK;
+}
+
+template <class L, int ST>
+static int step_dispatch(const StepArgs& a, int variant, int threads, cudaStream_t s)
+{
+    return launch_step<L, ST>(a, variant, threads, s);
+}
+
+extern "C" int lbm_step_pull(const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
+                             const lbm_launch_t* launch, const uint8_t* kind, const void* f_src, void* f_dst,
+                             lbm_stream_t stream)
+{
+    if (!grid_valid(g) || !p || !kind || !f_src || !f_dst || f_src == f_dst || !special_valid(sp, false))
+        return LBM_ERR_INVALID;
+    StepArgs a;
+    int threads = 0;
+    int st = make_args(a, g, p, sp, launch, kind, f_src, f_dst, threads);
+    if (st != LBM_OK) return st;
+    const int lattice = g->lattice, storage = g->storage;
+    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, LBM_PULL, threads, (cudaStream_t)stream); };
+    return record(run());
+}
+
+extern "C" int lbm_step_aa(const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
+                           const lbm_launch_t* launch, const uint8_t* kind, void* f, int32_t parity,
+                           lbm_stream_t stream)
+{
+    if (!grid_valid(g) || !p || !kind || !f || !special_valid(sp, true)) return LBM_ERR_INVALID;
+    if (parity != LBM_AA_EVEN && parity != LBM_AA_ODD) return LBM_ERR_INVALID;
+    StepArgs a;
+    int threads = 0;
+    int st = make_args(a, g, p, sp, launch, kind, f, f, threads);
+    if (st != LBM_OK) return st;
+    const int lattice = g->lattice, storage = g->storage;
+    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, parity, threads, (cudaStream_t)stream); };
+    return record(run());
+}
+
+template <class L, int ST>
+static int resources_dispatch(int which, int32_t* out4)
+{
+    return step_resources<L, ST>(which, out4);
+}
+
+extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t which, int32_t* out4)
+{
+    if (!out4) return LBM_ERR_INVALID;
+    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, resources_dispatch, which, out4); };
+    return record(run());
+}
+
+extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
+
+extern "C" int32_t lbm_abi_version(void) { return 1; }

@@ -1,0 +1,4 @@
+// Step kernel instantiations for D3Q19, bf16 storage.
+#include "step_kernels.cuh"
+
+LBM_INSTANTIATE_STEP(D3Q19, LBM_BF16)

@@ -1,0 +1,249 @@
+// The fused LBM time step: two-lattice pull and in-place AA, D2Q9/D3Q19,
+// float32/float64/float16/bfloat16 storage.
+//
+// One launch updates every fluid node once:
+//   * bulk blocks: a (tile_x x tile_y) tile of one z plane, one node per
+//     thread. A thread reads its kind byte; SOLID and SPECIAL nodes return,
+//     NEAR nodes test the kind of each source (bounce-back), every other node
+//     streams with no branch at all.
+//   * boundary warps: the blocks after the bulk range walk the compact list
+//     of SPECIAL nodes (link rules, immersed-boundary force, AA rule-term
+//     exports). They run the same per-node code with the rule and force
+//     look-ups switched on, so rules need no separate pre-pass launch.
+//
+// Race freedom.
+//   Pull: f_src is never written; rules read it directly.
+//   AA (reference kernels/stream_collide_aa.cu:15-28): in the odd step the
+//   thread of node x reads slot (opp i, x - c_i) and writes (i, x + c_i);
+//   both belong to x alone, bounce-back slots included. A rule, however,
+//   reads populations of other nodes, which the same launch overwrites. The
+//   AA kernels therefore never read rule terms from the lattice: every
+//   node that a rule term refers to is a SPECIAL exporter whose thread
+//   copies f*_k (rounded to the storage format) into export_out after its
+//   collision, and the next launch evaluates its rules from that copy
+//   (export_in). The two export buffers alternate between launches.
+#pragma once
+
+#include "lbm_common.cuh"
+
+namespace lbm {
+
+template <class L, int ST, int VAR>
+struct StepKernel {
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    static constexpr int Q = L::Q;
+
+    __device__ static __forceinline__ R rule_value(const StepArgs& a, int r)
+    {
+        const lbm_special_t& sp = a.sp;
+        const R* __restrict__ coeff = static_cast<const R*>(sp.term_coeff);
+        R v = static_cast<const R*>(sp.rule_const)[r];
+        const int t1 = sp.term_start[r + 1];
+        if (VAR == LBM_PULL) {
+            const T* __restrict__ f = static_cast<const T*>(a.f_src);
+            for (int t = sp.term_start[r]; t < t1; ++t) {
+                const int64_t slot = (int64_t)sp.term_dir[t] * a.qstride + sp.term_node[t];
+                v += coeff[t] * S::load(f + slot);
+            }
+        } else {
+            const R* __restrict__ ex = static_cast<const R*>(sp.export_in);
+            for (int t = sp.term_start[r]; t < t1; ++t) v += coeff[t] * ex[sp.term_export[t]];
+        }
+        return v;
+    }
+
+    template <bool SPECIAL>
+    __device__ static __forceinline__ void node(const StepArgs& a, int x, int y, int z, int64_t nd, bool near, int64_t s)
+    {
+        const uint8_t* __restrict__ kind = a.kind;
+        const int64_t qs = a.qstride;
+        const R* __restrict__ wall = static_cast<const R*>(a.wall_u);
+        uint32_t rmask = 0;
+        int rfirst = 0;
+        if (SPECIAL) {
+            rmask = a.sp.rule_mask[s];
+            rfirst = a.sp.rule_first[s];
+        }
+        const int xm = wrap(x - 1, a.nx), xp = wrap(x + 1, a.nx);
+        const int ym = wrap(y - 1, a.ny), yp = wrap(y + 1, a.ny);
+        const int zm = L::D == 3 ? wrap(z - 1, a.nz) : 0, zp = L::D == 3 ? wrap(z + 1, a.nz) : 0;
+
+        R f[Q];
+        // ---- gather the streamed populations
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            if (VAR == LBM_AA_EVEN) {
+                f[i] = S::load(static_cast<const T*>(a.f_src) + i * qs + nd);
+                continue;
+            }
+            // source node x - c_i
+            const int sx = L::cx(i) > 0 ? xm : (L::cx(i) < 0 ? xp : x);
+            const int sy = L::cy(i) > 0 ? ym : (L::cy(i) < 0 ? yp : y);
+            const int sz = L::cz(i) > 0 ? zm : (L::cz(i) < 0 ? zp : z);
+            const int64_t src = ((int64_t)sz * a.ny + sy) * a.pitch + sx;
+            const T* fs = static_cast<const T*>(a.f_src);
+            if (i != 0 && near && (kind[src] & KIND_SOLID)) {
+                // halfway bounce-back: the population that left x towards the wall
+                const int slot = VAR == LBM_PULL ? L::opp(i) : i;
+                f[i] = S::load(fs + slot * qs + nd) + wall_term<L, R>(i, wall, src, qs);
+            } else if (VAR == LBM_PULL) {
+                f[i] = S::load_nc(fs + i * qs + src);
+            } else {
+                f[i] = S::load(fs + L::opp(i) * qs + src);
+            }
+        }
+
+        // ---- link rules replace the bounce-back value of their links. One
+        // loop over the set bits keeps a single copy of the term loop; the
+        // unrolled select writes the value without indexing f[] at run time.
+        if (SPECIAL) {
+            uint32_t m = rmask;
+            int r = rfirst;
+            while (m) {
+                const int i = __ffs(m) - 1;
+                m &= m - 1u;
+                const R v = rule_value(a, r++);
+#pragma unroll
+                for (int j = 0; j < Q; ++j)
+                    if (j == i) f[j] = v;
+            }
+        }
+
+        // ---- collide
+        R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
+        if (a.force_field != nullptr) {
+            const R* ff = static_cast<const R*>(a.force_field);
+            Fx += ff[nd];
+            Fy += ff[qs + nd];
+            if (L::D == 3) Fz += ff[2 * qs + nd];
+        }
+        if (SPECIAL) {
+            const int fs = a.sp.force_slot[s];
+            if (fs >= 0) {
+                const R* lf = static_cast<const R*>(a.sp.local_force);
+                const int64_t n = a.sp.n_local;
+                Fx += lf[fs];
+                Fy += lf[n + fs];
+                if (L::D == 3) Fz += lf[2 * n + fs];
+            }
+        }
+        collide<L, R>(f, R(a.wp), R(a.wm), Fx, Fy, Fz);
+
+        // ---- store
+        T* fd = static_cast<T*>(a.f_dst);
+        if (VAR == LBM_PULL) {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) S::store(fd + i * qs + nd, f[i]);
+        } else if (VAR == LBM_AA_EVEN) {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) S::store(fd + L::opp(i) * qs + nd, f[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) {
+                const int dx = L::cx(i) > 0 ? xp : (L::cx(i) < 0 ? xm : x);
+                const int dy = L::cy(i) > 0 ? yp : (L::cy(i) < 0 ? ym : y);
+                const int dz = L::cz(i) > 0 ? zp : (L::cz(i) < 0 ? zm : z);
+                const int64_t dst = ((int64_t)dz * a.ny + dy) * a.pitch + dx;
+                if (i != 0 && near && (kind[dst] & KIND_SOLID)) {
+                    S::store(fd + L::opp(i) * qs + nd, f[i] + wall_term<L, R>(L::opp(i), wall, dst, qs));
+                } else {
+                    S::store(fd + i * qs + dst, f[i]);
+                }
+            }
+        }
+
+        // ---- AA rule-term exports
+        if (SPECIAL && VAR != LBM_PULL) {
+            const uint32_t emask = a.sp.export_mask[s];
+            if (emask) {
+                R* out = static_cast<R*>(a.sp.export_out);
+                int e = a.sp.export_first[s];
+                uint32_t m = emask;
+                while (m) {
+                    const int k = __ffs(m) - 1;
+                    m &= m - 1u;
+                    R v = f[0];
+#pragma unroll
+                    for (int j = 1; j < Q; ++j)
+                        if (j == k) v = f[j];
+                    out[e++] = S::round(v);
+                }
+            }
+        }
+    }
+};
+
+template <class L, int ST, int VAR>
+__global__ void __launch_bounds__(256) lbm_step_kernel(const StepArgs a)
+{
+    using K = StepKernel<L, ST, VAR>;
+    const int64_t b = blockIdx.x;
+    if (b < a.bulk_blocks) {
+        const int tx = threadIdx.x % a.tile_x;
+        const int ty = threadIdx.x / a.tile_x;
+        int64_t t = b;
+        const int bx = (int)(t % a.tiles_x);
+        t /= a.tiles_x;
+        const int by = (int)(t % a.tiles_y);
+        const int z = (int)(t / a.tiles_y);
+        const int x = bx * a.tile_x + tx;
+        const int y = by * a.tile_y + ty;
+        if (x >= a.nx || y >= a.ny) return;
+        const int64_t nd = ((int64_t)z * a.ny + y) * a.pitch + x;
+        const uint8_t k = a.kind[nd];
+        if (k & (KIND_SOLID | KIND_SPECIAL)) return;
+        K::template node<false>(a, x, y, z, nd, (k & KIND_NEAR) != 0, -1);
+    } else {
+        const int64_t s = (b - a.bulk_blocks) * (int64_t)blockDim.x + threadIdx.x;
+        if (s >= a.sp.n_special) return;
+        const int64_t nd = a.sp.node[s];
+        const int64_t row = nd / a.pitch;
+        const int x = (int)(nd - row * a.pitch);
+        const int y = (int)(row % a.ny);
+        const int z = (int)(row / a.ny);
+        K::template node<true>(a, x, y, z, nd, (a.kind[nd] & KIND_NEAR) != 0, s);
+    }
+}
+
+template <class L, int ST>
+int launch_step(const StepArgs& a, int variant, int threads, cudaStream_t stream)
+{
+    const int64_t special_blocks = (a.sp.n_special + threads - 1) / threads;
+    const int64_t blocks = a.bulk_blocks + special_blocks;
+    if (blocks <= 0) return LBM_OK;
+    if (blocks > 0x7fffffffLL) return LBM_ERR_INVALID;
+    switch (variant) {
+    case LBM_PULL: lbm_step_kernel<L, ST, LBM_PULL><<<(unsigned)blocks, threads, 0, stream>>>(a); break;
+    case LBM_AA_EVEN: lbm_step_kernel<L, ST, LBM_AA_EVEN><<<(unsigned)blocks, threads, 0, stream>>>(a); break;
+    case LBM_AA_ODD: lbm_step_kernel<L, ST, LBM_AA_ODD><<<(unsigned)blocks, threads, 0, stream>>>(a); break;
+    default: return LBM_ERR_INVALID;
+    }
+    return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+}
+
+template <class L, int ST>
+int step_resources(int variant, int32_t* out4)
+{
+    cudaFuncAttributes attr;
+    cudaError_t e;
+    switch (variant) {
+    case LBM_PULL: e = cudaFuncGetAttributes(&attr, lbm_step_kernel<L, ST, LBM_PULL>); break;
+    case LBM_AA_EVEN: e = cudaFuncGetAttributes(&attr, lbm_step_kernel<L, ST, LBM_AA_EVEN>); break;
+    case LBM_AA_ODD: e = cudaFuncGetAttributes(&attr, lbm_step_kernel<L, ST, LBM_AA_ODD>); break;
+    default: return LBM_ERR_INVALID;
+    }
+    if (e != cudaSuccess) return LBM_ERR_LAUNCH;
+    out4[0] = attr.numRegs;
+    out4[1] = (int32_t)attr.localSizeBytes;
+    out4[2] = (int32_t)attr.sharedSizeBytes;
+    out4[3] = attr.maxThreadsPerBlock;
+    return LBM_OK;
+}
+
+}  // namespace lbm
+
+#define LBM_INSTANTIATE_STEP(L, ST)                                                        \
+    template int lbm::launch_step<lbm::L, ST>(const lbm::StepArgs&, int, int, cudaStream_t); \
+    template int lbm::step_resources<lbm::L, ST>(int, int32_t*);

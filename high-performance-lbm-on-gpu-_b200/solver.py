@@ -1,0 +1,684 @@
+"""Solver contract and the CUDA solver (the drop-in ``cuda`` backend).
+
+``Solver`` keeps the reference's driver semantics (``src/lbm/solver.py:61-221``):
+``run`` advances in chunks of ``check_every``/``every`` steps, checks for
+divergence after every chunk and fires the callback. ``CudaSolver`` holds the
+populations in PyTorch CUDA tensors and advances them with the fused sm_100a
+kernels of ``liblbm_b200.so``; nothing here computes on the CPU except input
+preparation (rule tables, geometry) and unit conversion of readouts.
+
+Backends (reference ``src/lbm/backends/__init__.py:23``):
+
+==============  ===========================================================
+``cuda``        two-lattice fused pull kernel (same as ``cuda-naive``)
+``cuda-naive``  two-lattice fused pull kernel
+``cuda-aa``     in-place AA pair (one lattice, steps in pairs)
+==============  ===========================================================
+"""
+
+from __future__ import annotations
+
+import functools
+import math
+from abc import ABC, abstractmethod
+from collections.abc import Callable
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .diagnostics import MacroscopicFields
+from .lattice import as_lattice
+from .params import COMPUTE_DTYPE
+
+DEFAULT_CHECK_EVERY = 500
+DEFAULT_BLOCK = (32, 8)
+BACKENDS = ("cuda", "cuda-naive", "cuda-aa")
+VARIANTS = ("pull", "aa")
+
+
+class BackendUnavailable(RuntimeError):
+    """The CUDA backend needs a CUDA device and the built library; one is missing."""
+
+
+class SimulationDiverged(RuntimeError):
+    """Non-finite populations or rho <= 0 at a fluid node (reference ``solver.py:39-51``)."""
+
+    def __init__(self, step: int, location: tuple[int, ...], reason: str):
+        self.step = step
+        self.location = location
+        names = "(y, x)" if len(location) == 2 else "(z, y, x)"
+        super().__init__(f"simulation diverged by step {step}: {reason} at node {names}={location}")
+
+
+@functools.cache
+def gpu_available() -> bool:
+    try:
+        import torch
+
+        if not torch.cuda.is_available() or torch.cuda.device_count() == 0:
+            return False
+        N.load()
+    except (ImportError, N.NativeUnavailable):
+        return False
+    return True
+
+
+def available_backends() -> tuple[str, ...]:
+    return BACKENDS if gpu_available() else ()
+
+
+def make_solver(params, backend: str = "cuda", **options) -> CudaSolver:
+    """Create a solver for ``params`` (reference ``backends/__init__.py:62-83``).
+
+    ``options`` go to ``CudaSolver`` (``block=``, ``force_field=``, ``graph=``...).
+    """
+    if backend not in BACKENDS:
+        raise ValueError(f"unknown backend {backend!r}; choose from {BACKENDS}")
+    return CudaSolver(params, variant="aa" if backend == "cuda-aa" else "pull", **options)
+
+
+class Solver(ABC):
+    """Driver shared by the CUDA variants: chunked run loop, watchdog, callbacks."""
+
+    step_multiple = 1
+    state_layout = "pull"
+
+    def __init__(self, params):
+        self.params = params
+        self.time_step = 0
+
+    @abstractmethod
+    def initialize(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0) -> None: ...
+
+    @abstractmethod
+    def _advance(self, steps: int) -> None: ...
+
+    @abstractmethod
+    def _check_health(self) -> None: ...
+
+    def run(self, steps: int, *, every: int = 0, callback: Callable | None = None,
+            check_every: int = DEFAULT_CHECK_EVERY) -> None:
+        """Advance ``steps`` steps (reference ``solver.py:119-160``, same chunking and errors)."""
+        if steps < 0 or every < 0 or check_every <= 0:
+            raise ValueError(f"need steps >= 0, every >= 0, check_every > 0; got {steps}, {every}, {check_every}")
+        m = self.step_multiple
+        if steps % m or every % m or check_every % m:
+            raise ValueError(
+                f"{type(self).__name__} advances in multiples of {m} steps; "
+                f"steps, every and check_every must be multiples of {m}"
+            )
+        done = 0
+        while done < steps:
+            stop = min(steps, (done // check_every + 1) * check_every)
+            if every:
+                stop = min(stop, (done // every + 1) * every)
+            self._advance(stop - done)
+            self.time_step += stop - done
+            done = stop
+            self._check_health()
+            if callback is not None and ((every and done % every == 0) or done == steps):
+                callback(self)
+
+
+# ---------------------------------------------------------------------------- device tables
+
+
+@dataclass
+class _SpecialTables:
+    """Device form of the boundary-warp work list (see ``lbm_special_t``)."""
+
+    tensors: dict
+    n_special: int
+    n_rules: int
+    n_terms: int
+    n_export: int
+    n_local: int
+
+
+def _pitched_index(flat: np.ndarray, shape: tuple[int, ...], pitch: int) -> np.ndarray:
+    """Natural flat node index -> pitched index (x row padded to ``pitch``)."""
+    flat = np.asarray(flat, dtype=np.int64)
+    nx = shape[-1]
+    return (flat // nx) * pitch + flat % nx
+
+
+def _natural_index(pitched: int, shape: tuple[int, ...], pitch: int) -> tuple[int, ...]:
+    row, x = divmod(int(pitched), pitch)
+    if len(shape) == 2:
+        return (row, x)
+    z, y = divmod(row, shape[1])
+    return (z, y, x)
+
+
+class CudaSolver(Solver):
+    """Fused stream-bounce-collide on a B200 (reference ``backends/cuda_solver.py:179-326``).
+
+    Args:
+        params: a ``SimulationParams`` (this package's or the reference's).
+        variant: ``"pull"`` (two lattices) or ``"aa"`` (in place, steps in pairs).
+        block: bulk tile (x, y) in threads; x a multiple of 32, at most 256 threads.
+        force_field: optional per-node Guo force (d, *shape) added to the uniform force.
+        graph: capture chunks of steps in CUDA graphs (saves launch latency on small grids).
+        device: CUDA device (default: current).
+    """
+
+    def __init__(self, params, variant: str = "pull", block=DEFAULT_BLOCK, force_field=None,
+                 graph: bool = True, device=None, pitch: int | None = None):
+        if variant not in VARIANTS:
+            raise ValueError(f"unknown CUDA variant {variant!r}; choose from {VARIANTS}")
+        bx, by = (int(b) for b in block)
+        if bx <= 0 or by <= 0 or bx * by > 1024:
+            raise ValueError(f"block must be positive with at most 1024 threads; got {block}")
+        if bx % 32 or bx * by > 256:
+            raise ValueError(f"block x must be a multiple of 32 and block at most 256 threads; got {block}")
+        try:
+            import torch
+        except ImportError as exc:  # pragma: no cover
+            raise BackendUnavailable("PyTorch is required for the CUDA backend") from exc
+        if not torch.cuda.is_available():
+            raise BackendUnavailable("no CUDA device found")
+        try:
+            N.load()
+        except N.NativeUnavailable as exc:
+            raise BackendUnavailable(str(exc)) from exc
+        super().__init__(params)
+        self.torch = torch
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.variant = variant
+        self.step_multiple = 2 if variant == "aa" else 1
+        self.use_graph = bool(graph)
+        self._graphs: dict = {}
+
+        lattice = as_lattice(params.lattice)
+        self.lattice = lattice
+        d, q = lattice.d, lattice.q
+        shape = tuple(params.shape)
+        self.shape = shape
+        self.n_nodes = math.prod(shape)
+        nx = shape[-1]
+        ny = shape[-2]
+        nz = shape[0] if d == 3 else 1
+        self.pitch = int(pitch) if pitch is not None else nx
+        if self.pitch < nx:
+            raise ValueError(f"pitch must be >= nx={nx}; got {self.pitch}")
+        self.qstride = self.pitch * ny * nz
+        self.storage = params.dtype
+        self.compute = COMPUTE_DTYPE[params.dtype]
+        tdt = {"float32": torch.float32, "float64": torch.float64, "float16": torch.float16, "bfloat16": torch.bfloat16}
+        self.t_store = tdt[self.storage]
+        self.t_real = tdt[self.compute]
+        self.grid = N.Grid(N.LATTICE_CODE[lattice.name], N.STORAGE_CODE[self.storage], nx, ny, nz, self.pitch, self.qstride)
+        self.launch = N.Launch(bx, by)
+        self.block = (bx, by)
+
+        # ---- physics
+        wp, wm = params.relaxation_rates
+        force = tuple(float(v) for v in params.force) + (0.0,) * (3 - d)
+        wall = np.asarray(params.wall_velocity, dtype=np.float64)
+        self._wall = self._upload_field(wall) if np.any(wall != 0.0) else None
+        self._force_field = None
+        if force_field is not None:
+            self._force_field = self._upload_field(np.asarray(force_field, dtype=np.float64).reshape(d, *shape))
+        self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field))
+
+        # ---- immersed boundary and link rules -> special nodes
+        self._ibm = None
+        if params.immersed is not None:
+            from .ibm import build_tables
+
+            if force_field is not None:
+                raise ValueError("a per-node force field cannot be combined with an immersed body")
+            self._ibm = _IbmState(self, build_tables(params.immersed, lattice, np.asarray(params.solid)))
+        self._special = self._build_special(params)
+
+        # ---- node kinds
+        solid = self._upload_scalar(np.asarray(params.solid, dtype=np.uint8), torch.uint8)
+        self._kind = torch.empty(self.qstride, dtype=torch.uint8, device=self.device)
+        sp_nodes = self._special.tensors.get("node")
+        self._native("lbm_classify", N.C.byref(self.grid), N.ptr(solid), N.ptr(sp_nodes), self._special.n_special,
+                     N.ptr(self._kind), self._stream())
+        self._solid_host = np.asarray(params.solid, dtype=bool)
+
+        # ---- populations
+        self._f = torch.empty((q, self.qstride), dtype=self.t_store, device=self.device)
+        self._f_next = torch.empty_like(self._f) if variant == "pull" else None
+        self._health = torch.empty(2, dtype=torch.int64, device=self.device)
+        self.initialize()
+
+    # ------------------------------------------------------------------ helpers
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.device).cuda_stream
+
+    def _native(self, name, *args):
+        N.call(name, *args)
+
+    def _to_pitched(self, host: np.ndarray, dtype):
+        """(..., *shape) host array -> device tensor (..., qstride), zero padding columns."""
+        torch = self.torch
+        host = np.ascontiguousarray(host)
+        lead = host.shape[: host.ndim - len(self.shape)]
+        t = torch.from_numpy(host).to(self.device, dtype)
+        if self.pitch == self.shape[-1]:
+            return t.reshape(*lead, self.qstride).contiguous()
+        out = torch.zeros((*lead, *self.shape[:-1], self.pitch), dtype=dtype, device=self.device)
+        out[..., : self.shape[-1]] = t
+        return out.reshape(*lead, self.qstride)
+
+    def _from_pitched(self, t):
+        """Device tensor (..., qstride) -> host array (..., *shape)."""
+        lead = t.shape[:-1]
+        view = t.reshape(*lead, *self.shape[:-1], self.pitch)[..., : self.shape[-1]]
+        return view.contiguous().cpu().numpy()
+
+    def _upload_field(self, host):
+        return self._to_pitched(np.asarray(host, dtype=np.float64), self.t_real)
+
+    def _upload_scalar(self, host, dtype):
+        return self._to_pitched(host, dtype)
+
+    def _pitched(self, flat):
+        return _pitched_index(flat, self.shape, self.pitch)
+
+    # ------------------------------------------------------------------ special nodes
+    def _build_special(self, params) -> _SpecialTables:
+        torch = self.torch
+        lat = self.lattice
+        n = self.n_nodes
+        rules = params.link_rules
+        rule_nodes = np.zeros(0, dtype=np.int64)
+        t = {}
+        n_rules = n_terms = n_export = 0
+        if rules is not None and len(rules):
+            node = np.asarray(rules.node, dtype=np.int64)
+            direction = np.asarray(rules.direction, dtype=np.int64)
+            v = rules.values
+            coeff = np.asarray(v.coeff, dtype=np.float64)
+            tdir = np.asarray(v.direction, dtype=np.int64)
+            tnode = np.asarray(v.node, dtype=np.int64)
+            const = np.asarray(v.constant, dtype=np.float64)
+            order = np.lexsort((direction, node))
+            node, direction = node[order], direction[order]
+            coeff, tdir, tnode, const = coeff[order], tdir[order], tnode[order], const[order]
+            live = coeff != 0.0
+            counts = live.sum(axis=1)
+            start = np.zeros(len(node) + 1, dtype=np.int64)
+            np.cumsum(counts, out=start[1:])
+            term_dir = tdir[live]
+            term_node = tnode[live]
+            term_coeff = coeff[live]
+            n_rules, n_terms = len(node), int(start[-1])
+            if n_terms >= 2**31:
+                raise ValueError("too many rule terms")
+            if np.any(term_node < 0) or np.any(term_node >= n) or np.any(term_dir < 0) or np.any(term_dir >= lat.q):
+                raise ValueError("a rule term points outside the lattice")
+            rule_nodes = node
+            t["term_start"] = torch.from_numpy(start.astype(np.int32)).to(self.device)
+            t["rule_const"] = torch.from_numpy(const).to(self.device, self.t_real)
+            t["term_dir"] = torch.from_numpy(term_dir.astype(np.int32)).to(self.device)
+            t["term_node"] = torch.from_numpy(self._pitched(term_node)).to(self.device)
+            t["term_coeff"] = torch.from_numpy(term_coeff).to(self.device, self.t_real)
+            rule_dir = direction
+        ibm_nodes = self._ibm.tables.nodes if self._ibm is not None else np.zeros(0, dtype=np.int64)
+        export_nodes = np.zeros(0, dtype=np.int64)
+        if self.variant == "aa" and n_rules:
+            solid = np.asarray(params.solid, dtype=bool).ravel()
+            if np.any(solid[term_node]):
+                raise ValueError("the AA variant needs every rule term on a fluid node")
+            keys = term_node * 32 + term_dir
+            ukeys, term_export = np.unique(keys, return_inverse=True)
+            n_export = ukeys.size
+            export_nodes = ukeys // 32
+            export_dirs = ukeys % 32
+            t["term_export"] = torch.from_numpy(term_export.astype(np.int32)).to(self.device)
+        nodes = np.unique(np.concatenate([rule_nodes, ibm_nodes, export_nodes]))
+        ns = nodes.size
+        if ns == 0:
+            return _SpecialTables({}, 0, 0, 0, 0, 0)
+        rule_mask = np.zeros(ns, dtype=np.uint32)
+        rule_first = np.zeros(ns, dtype=np.int32)
+        if n_rules:
+            # rules are sorted by (node, direction): a node's rules start at its first occurrence
+            pos = np.searchsorted(nodes, rule_nodes)
+            np.bitwise_or.at(rule_mask, pos, (np.uint32(1) << rule_dir.astype(np.uint32)))
+            rule_first = np.searchsorted(rule_nodes, nodes, side="left").astype(np.int32)
+        force_slot = np.full(ns, -1, dtype=np.int32)
+        if ibm_nodes.size:
+            force_slot[np.searchsorted(nodes, ibm_nodes)] = np.arange(ibm_nodes.size, dtype=np.int32)
+        export_mask = np.zeros(ns, dtype=np.uint32)
+        export_first = np.zeros(ns, dtype=np.int32)
+        if n_export:
+            pos = np.searchsorted(nodes, export_nodes)
+            np.bitwise_or.at(export_mask, pos, (np.uint32(1) << export_dirs.astype(np.uint32)))
+            # exports are sorted by (node, direction) through their keys
+            export_first = np.searchsorted(export_nodes, nodes, side="left").astype(np.int32)
+            t["export_a"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
+            t["export_b"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
+        t["node"] = torch.from_numpy(self._pitched(nodes)).to(self.device)
+        t["rule_mask"] = torch.from_numpy(rule_mask.view(np.int32)).to(self.device)
+        t["rule_first"] = torch.from_numpy(rule_first).to(self.device)
+        t["force_slot"] = torch.from_numpy(force_slot).to(self.device)
+        t["export_mask"] = torch.from_numpy(export_mask.view(np.int32)).to(self.device)
+        t["export_first"] = torch.from_numpy(export_first).to(self.device)
+        return _SpecialTables(t, ns, n_rules, n_terms, n_export, int(ibm_nodes.size))
+
+    def _special_struct(self, export_in=None, export_out=None) -> N.Special:
+        s = self._special
+        t = s.tensors
+        g = t.get
+        local = self._ibm.final_force if self._ibm is not None else None
+        return N.Special(
+            s.n_special, N.ptr(g("node")), N.ptr(g("rule_mask")), N.ptr(g("rule_first")), N.ptr(g("force_slot")),
+            N.ptr(g("export_mask")), N.ptr(g("export_first")), s.n_rules, s.n_terms, N.ptr(g("term_start")),
+            N.ptr(g("rule_const")), N.ptr(g("term_dir")), N.ptr(g("term_node")), N.ptr(g("term_export")),
+            N.ptr(g("term_coeff")), N.ptr(local), s.n_local, s.n_export, N.ptr(export_in), N.ptr(export_out),
+        )
+
+    # ------------------------------------------------------------------ state
+    @property
+    def xp(self):
+        return self.torch
+
+    @property
+    def lattice_bytes(self) -> int:
+        """Device memory held by the population buffers (reference ``cuda_solver.py:251-256``)."""
+        buffers = 1 if self.variant == "aa" else 2
+        return buffers * self.lattice.q * self.n_nodes * self.t_store.itemsize
+
+    @property
+    def state_layout(self) -> str:
+        return "aa_odd" if self.variant == "aa" else "pull"
+
+    @property
+    def _layout_code(self) -> int:
+        return N.LAYOUT_AA_ODD if self.variant == "aa" else N.LAYOUT_PULL
+
+    def _field_f64(self, value, lead: tuple[int, ...] = ()):
+        """Scalar, host array or tensor broadcast to (*lead, *shape) -> float64 device (*lead, qstride)."""
+        torch = self.torch
+        shape = (*lead, *self.shape)
+        if isinstance(value, torch.Tensor):
+            t = value.to(self.device, torch.float64, non_blocking=True)
+        else:
+            arr = np.asarray(value, dtype=np.float64)
+            if arr.ndim == 0:
+                return torch.full((*lead, self.qstride), float(arr), dtype=torch.float64, device=self.device)
+            t = torch.from_numpy(np.ascontiguousarray(arr)).to(self.device, non_blocking=True)
+        t = t.expand(shape)
+        if self.pitch == self.shape[-1]:
+            return t.reshape(*lead, self.qstride).contiguous()
+        out = torch.zeros((*shape[:-1], self.pitch), dtype=torch.float64, device=self.device)
+        out[..., : self.shape[-1]] = t
+        return out.reshape(*lead, self.qstride)
+
+    def initialize(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0) -> None:
+        """Equilibrium with u + F/(2 rho), combined in float64 on the device (reference ``solver.py:101-117``).
+
+        Fields may be scalars, NumPy arrays or torch tensors (pinned host
+        tensors are copied asynchronously).
+        """
+        torch = self.torch
+        d = self.lattice.d
+        if d == 2 and bool(np.any(np.asarray(uz.cpu() if hasattr(uz, "cpu") else uz) != 0)):
+            raise ValueError("a 2D simulation has no z velocity; leave uz at 0")
+        rho_t = self._field_f64(rho)
+        comps = (ux, uy, uz)[:d]
+        u_t = torch.stack([self._field_f64(c) for c in comps])
+        self._native("lbm_init_equilibrium", N.C.byref(self.grid), N.C.byref(self.physics), N.ptr(rho_t), N.ptr(u_t),
+                     self._layout_code, N.ptr(self._f), self._stream())
+        if self._f_next is not None:
+            self._f_next.copy_(self._f)
+        self._after_state_change()
+        self.time_step = 0
+
+    def set_populations(self, f) -> None:
+        """Population-exact restore from natural order (q, *shape) (host array or tensor)."""
+        torch = self.torch
+        q = self.lattice.q
+        if isinstance(f, torch.Tensor):
+            f = f.detach().cpu().numpy()
+        f = np.asarray(f, dtype=np.float64)
+        if f.shape != (q, *self.shape):
+            raise ValueError(f"populations must have shape {(q, *self.shape)}; got {f.shape}")
+        nat = self._to_pitched(f.astype(self.compute), self.t_real)
+        self._native("lbm_pack", N.C.byref(self.grid), N.ptr(nat), self._layout_code, N.ptr(self._f), self._stream())
+        if self._f_next is not None:
+            self._f_next.copy_(self._f)
+        self._after_state_change()
+
+    def _after_state_change(self):
+        s = self._special
+        if self.variant == "aa" and s.n_export:
+            self._export_cur = s.tensors["export_a"]
+            self._export_nxt = s.tensors["export_b"]
+            sp = self._special_struct()
+            self._native("lbm_export_prime", N.C.byref(self.grid), N.C.byref(sp), N.ptr(self._f), N.LAYOUT_AA_ODD,
+                         N.ptr(self._export_cur), self._stream())
+        self._graphs.clear()
+
+    def _natural_populations(self):
+        """Device tensor (q, qstride) of f*_i in natural order, compute dtype."""
+        out = self.torch.empty((self.lattice.q, self.qstride), dtype=self.t_real, device=self.device)
+        self._native("lbm_unpack", N.C.byref(self.grid), N.ptr(self._f), self._layout_code, N.ptr(out), self._stream())
+        return out
+
+    def _device_populations(self):
+        """Post-collision populations in natural order, (q, *shape) torch tensor (compute dtype)."""
+        t = self._natural_populations()
+        view = t.reshape(self.lattice.q, *self.shape[:-1], self.pitch)[..., : self.shape[-1]]
+        return view
+
+    def populations(self) -> np.ndarray:
+        """Host copy of f~* in natural order, shape (q, *shape) (reference ``solver.py:190-192``)."""
+        return self._from_pitched(self._natural_populations())
+
+    def _state_buffer(self):
+        return self._f
+
+    # ------------------------------------------------------------------ stepping
+    def _launch_pull(self):
+        if self._ibm is not None:
+            self._ibm.run(self._f, N.LAYOUT_PULL)
+        sp = self._special_struct()
+        self._native("lbm_step_pull", N.C.byref(self.grid), N.C.byref(self.physics), N.C.byref(sp), N.C.byref(self.launch),
+                     N.ptr(self._kind), N.ptr(self._f), N.ptr(self._f_next), self._stream())
+        self._f, self._f_next = self._f_next, self._f
+
+    def _launch_aa(self, parity, layout):
+        if self._ibm is not None:
+            self._ibm.run(self._f, layout)
+        ex_in = ex_out = None
+        if self._special.n_export:
+            ex_in, ex_out = self._export_cur, self._export_nxt
+        sp = self._special_struct(ex_in, ex_out)
+        self._native("lbm_step_aa", N.C.byref(self.grid), N.C.byref(self.physics), N.C.byref(sp), N.C.byref(self.launch),
+                     N.ptr(self._kind), N.ptr(self._f), parity, self._stream())
+        if self._special.n_export:
+            self._export_cur, self._export_nxt = self._export_nxt, self._export_cur
+
+    def _launch_steps(self, steps: int):
+        if self.variant == "aa":
+            for _ in range(steps // 2):
+                self._launch_aa(N.LBM_AA_ODD, N.LAYOUT_AA_ODD)
+                self._launch_aa(N.LBM_AA_EVEN, N.LAYOUT_AA_EVEN)
+        else:
+            for _ in range(steps):
+                self._launch_pull()
+
+    GRAPH_CHUNK = 32
+
+    def _advance(self, steps: int) -> None:
+        if steps <= 0:
+            return
+        if not self.use_graph or steps < self.GRAPH_CHUNK:
+            self._launch_steps(steps)
+            return
+        chunk = self.GRAPH_CHUNK
+        graph = self._graph(chunk)
+        for _ in range(steps // chunk):
+            graph.replay()
+        self._launch_steps(steps % chunk)
+
+    def _graph(self, chunk: int):
+        """A CUDA graph of ``chunk`` steps; it leaves every buffer pointer where it found it."""
+        key = (chunk, self._f.data_ptr())
+        graph = self._graphs.get(key)
+        if graph is not None:
+            return graph
+        torch = self.torch
+        f0, f1 = self._f, self._f_next
+        ex = (getattr(self, "_export_cur", None), getattr(self, "_export_nxt", None))
+        stream = torch.cuda.Stream(self.device)
+        stream.wait_stream(torch.cuda.current_stream(self.device))
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            graph.capture_begin()
+            try:
+                self._launch_steps(chunk)
+            finally:
+                graph.capture_end()
+        torch.cuda.current_stream(self.device).wait_stream(stream)
+        # Capture only recorded the launches; restore the pointer rotation.
+        self._f, self._f_next = f0, f1
+        self._export_cur, self._export_nxt = ex
+        self._graphs[key] = graph
+        return graph
+
+    def synchronize(self) -> None:
+        self.torch.cuda.synchronize(self.device)
+
+    # ------------------------------------------------------------------ readouts
+    def _check_health(self) -> None:
+        """Device watchdog (reference ``solver.py:162-172``); raises ``SimulationDiverged``."""
+        self._native("lbm_health_reset", N.ptr(self._health), self._stream())
+        self._native("lbm_health", N.C.byref(self.grid), N.ptr(self._kind), N.ptr(self._f), N.ptr(self._health), self._stream())
+        first, nonfinite = (int(v) for v in self._health.cpu().tolist())
+        if first == 2**63 - 1:
+            return
+        location = _natural_index(first, self.shape, self.pitch)
+        reason = "non-finite populations" if nonfinite else "non-positive density"
+        raise SimulationDiverged(self.time_step, location, reason)
+
+    def macroscopic(self) -> MacroscopicFields:
+        """rho and u on the host (reference ``solver.py:209-221``)."""
+        torch = self.torch
+        d = self.lattice.d
+        rho = torch.empty(self.qstride, dtype=self.t_real, device=self.device)
+        u = torch.empty((d, self.qstride), dtype=self.t_real, device=self.device)
+        local_nodes = local = None
+        n_local = 0
+        if self._ibm is not None:
+            local_nodes = self._ibm.node
+            local = self._ibm.final_force
+            n_local = self._ibm.tables.n_nodes
+        self._native("lbm_macroscopic", N.C.byref(self.grid), N.C.byref(self.physics), N.ptr(self._kind), N.ptr(self._f),
+                     self._layout_code, N.ptr(local_nodes), N.ptr(local), n_local, N.ptr(rho), N.ptr(u), self._stream())
+        rho_h = self._from_pitched(rho)
+        u_h = self._from_pitched(u)
+        return MacroscopicFields(rho=rho_h, u=tuple(u_h[a] for a in range(d)), solid=np.array(self._solid_host))
+
+    def _device_slots(self, compiled):
+        slots = np.asarray(compiled.slots, dtype=np.int64)
+        k, node = np.divmod(slots, self.n_nodes)
+        return k * self.qstride + self._pitched(node)
+
+    def _affine_tensors(self, compiled):
+        torch = self.torch
+        coeff = np.asarray(compiled.coeff, dtype=np.float64)
+        if coeff.ndim == 1:
+            coeff = coeff[:, None]
+        slots = self._device_slots(compiled).reshape(coeff.shape)
+        const = np.asarray(compiled.constant, dtype=np.float64)
+        return (torch.from_numpy(np.ascontiguousarray(slots)).to(self.device),
+                torch.from_numpy(np.ascontiguousarray(coeff)).to(self.device),
+                torch.from_numpy(np.ascontiguousarray(const)).to(self.device), coeff.shape)
+
+    def evaluate_affine(self, compiled) -> np.ndarray:
+        """Host float64 values of compiled affine expressions (reference ``solver.py:178-188``)."""
+        slots, coeff, const, (rows, terms) = self._affine_tensors(compiled)
+        values = self.torch.empty(rows, dtype=self.torch.float64, device=self.device)
+        self._native("lbm_affine_gather", self.grid.storage, N.ptr(self._f), N.ptr(slots), N.ptr(coeff), N.ptr(const),
+                     rows, terms, N.ptr(values), self._stream())
+        return values.cpu().numpy()
+
+    def reduce_affine(self, compiled, weight) -> np.ndarray:
+        """sum_r weight[r] * value_r in float64 on the device (momentum-exchange force)."""
+        torch = self.torch
+        slots, coeff, const, (rows, terms) = self._affine_tensors(compiled)
+        weight = np.asarray(weight, dtype=np.float64).reshape(rows, -1)
+        d = weight.shape[1]
+        if rows == 0:
+            return np.zeros(d)
+        w = torch.from_numpy(np.ascontiguousarray(weight)).to(self.device)
+        blocks = (rows + 255) // 256
+        partial = torch.empty(blocks * d, dtype=torch.float64, device=self.device)
+        counter = torch.zeros(1, dtype=torch.int32, device=self.device)
+        out = torch.empty(d, dtype=torch.float64, device=self.device)
+        self._native("lbm_affine_reduce", self.grid.storage, N.ptr(self._f), N.ptr(slots), N.ptr(coeff), N.ptr(const),
+                     N.ptr(w), rows, terms, d, N.ptr(partial), N.ptr(counter), N.ptr(out), self._stream())
+        return out.cpu().numpy()
+
+    @property
+    def immersed_force(self) -> np.ndarray:
+        """Force on the immersed body during the last step, host float64 (reference ``solver.py:201-207``)."""
+        if self._ibm is None:
+            raise AttributeError("this simulation has no immersed body")
+        return self._ibm.body_force()
+
+    def kernel_resources(self) -> dict[str, dict[str, int]]:
+        """Registers, spill bytes and shared memory of the step kernels (``cuda_solver.py:311-326``)."""
+        lib = N.load()
+        which = {"aa_odd": N.LBM_AA_ODD, "aa_even": N.LBM_AA_EVEN} if self.variant == "aa" else {"stream_collide_pull": N.LBM_PULL}
+        out = {}
+        for name, code in which.items():
+            buf = (N.i32 * 4)()
+            N.check(lib.lbm_kernel_resources(self.grid.lattice, self.grid.storage, code, buf), "lbm_kernel_resources")
+            out[name] = {"registers": buf[0], "local_bytes": buf[1], "shared_bytes": buf[2], "max_threads": buf[3]}
+        return out
+
+
+class _IbmState:
+    """Device tables and scratch of the immersed-boundary kernels for one solver."""
+
+    def __init__(self, solver: CudaSolver, tables):
+        torch = solver.torch
+        dev, real = solver.device, solver.t_real
+        d = solver.lattice.d
+        self.solver = solver
+        self.tables = tables
+        self.d = d
+        to = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)  # noqa: E731
+        self.node = to(solver._pitched(tables.nodes), torch.int64)
+        self._t = {
+            "stencil": to(tables.stencil.astype(np.int32), torch.int32),
+            "weight": to(tables.weights, real),
+            "area": to(tables.areas, real),
+            "inv_start": to(tables.inv_start.astype(np.int32), torch.int32),
+            "inv_marker": to(tables.inv_marker.astype(np.int32), torch.int32),
+            "inv_weight": to(tables.inv_weight, real),
+            "rho": torch.zeros(tables.n_nodes, dtype=real, device=dev),
+            "u_star": torch.zeros((d, tables.n_nodes), dtype=real, device=dev),
+            "marker_force": torch.zeros((tables.iterations, d, tables.n_markers), dtype=real, device=dev),
+        }
+        self.force = [torch.zeros((d, tables.n_nodes), dtype=real, device=dev) for _ in range(2)]
+        self.final_force = self.force[(tables.iterations - 1) % 2]
+        self._body = torch.zeros(d, dtype=torch.float64, device=dev)
+        g = self._t.get
+        self.struct = N.Ibm(
+            tables.n_nodes, tables.n_markers, tables.stencil.shape[1], N.ptr(self.node), N.ptr(g("stencil")),
+            N.ptr(g("weight")), N.ptr(g("area")), N.ptr(g("inv_start")), N.ptr(g("inv_marker")),
+            N.ptr(g("inv_weight")), N.ptr(g("rho")), N.ptr(g("u_star")), N.ptr(g("marker_force")),
+        )
+
+    def run(self, f, layout: int) -> None:
+        s = self.solver
+        stream = s._stream()
+        N.call("lbm_ibm_moments", N.C.byref(s.grid), N.C.byref(s.physics), N.C.byref(self.struct), N.ptr(f), layout, stream)
+        for it in range(self.tables.iterations):
+            fin = None if it == 0 else self.force[(it - 1) % 2]
+            N.call("lbm_ibm_iteration", N.C.byref(s.grid), N.C.byref(self.struct), it, N.ptr(fin), N.ptr(self.force[it % 2]), stream)
+
+    def body_force(self) -> np.ndarray:
+        s = self.solver
+        N.call("lbm_ibm_body_force", N.C.byref(s.grid), N.C.byref(self.struct), self.tables.iterations, N.ptr(self._body), s._stream())
+        return self._body.cpu().numpy().astype(np.float64)

@@ -1,0 +1,310 @@
+"""NumPy restatement of the reference LBM step -- TEST INFRASTRUCTURE ONLY.
+
+Each function cites the reference file:line it restates (paths relative to the
+reference project). Written against plain NumPy; every array keeps the
+simulation dtype so float32 runs round like the reference's float32 runs.
+
+16-bit storage ("float16", "bfloat16") has no counterpart in the reference.
+The oracle emulates it: arithmetic in float32, populations rounded to the
+storage format after every step exactly as the CUDA kernels store them
+(``quantize``), so the GPU path can be checked bit-for-tolerance.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+FP16_SCALE = 2.0**14
+"""Power-of-two factor applied before rounding to float16 (keeps small f~ out of subnormals)."""
+
+
+class OracleDiverged(RuntimeError):
+    def __init__(self, step, location, reason):
+        self.step, self.location, self.reason = step, location, reason
+        super().__init__(f"simulation diverged by step {step}: {reason} at node {location}")
+
+
+def compute_dtype(dtype: str):
+    return np.float64 if dtype == "float64" else np.float32
+
+
+def quantize(f: np.ndarray, dtype: str) -> np.ndarray:
+    """Round float32 values to the storage format and back (no-op for float32/float64)."""
+    if dtype == "float16":
+        scaled = (f.astype(np.float32) * np.float32(FP16_SCALE)).astype(np.float16)
+        return scaled.astype(np.float32) * np.float32(1.0 / FP16_SCALE)
+    if dtype == "bfloat16":
+        bits = np.ascontiguousarray(f, dtype=np.float32).view(np.uint32).astype(np.uint64)
+        bias = 0x7FFF + ((bits >> 16) & 1)
+        rounded = ((bits + bias) & 0xFFFF0000).astype(np.uint32)
+        return rounded.view(np.float32)
+    return f
+
+
+def _dot(c, vec):
+    """c . vec skipping zero components (reference ``equilibrium.py:23-30``)."""
+    return sum(ca * va for ca, va in zip(c, vec, strict=True) if ca)
+
+
+def equilibrium(lattice, drho, u):
+    """Shifted 2nd-order equilibrium w_i [drho + rho (3cu + 4.5 (cu)^2 - 1.5 u.u)] (``equilibrium.py:40-58``)."""
+    rho = 1.0 + drho
+    usq = 1.5 * sum(ua * ua for ua in u)
+    out = []
+    for ci, wi in zip(lattice.c, lattice.w, strict=True):
+        cu = 3.0 * _dot(ci, u)
+        out.append(wi * (drho + rho * (cu + 0.5 * cu * cu - usq)))
+    return np.stack(out)
+
+
+def _momentum(lattice, f):
+    return tuple(
+        sum(ca * f[i] for i, ca in enumerate(lattice.component(a)) if ca) for a in range(lattice.d)
+    )
+
+
+def _is_zero(v) -> bool:
+    return isinstance(v, (int, float)) and v == 0.0
+
+
+def guo_source(lattice, u, force, wp, wm):
+    """Guo source split into even/odd parts (``forcing.py:37-56``)."""
+    u_dot_f = sum(ua * fa for ua, fa in zip(u, force, strict=True))
+    ap, am = 1.0 - 0.5 * wp, 1.0 - 0.5 * wm
+    out = []
+    for ci, wi in zip(lattice.c, lattice.w, strict=True):
+        cf = _dot(ci, force)
+        cu = _dot(ci, u)
+        out.append(wi * (ap * (9.0 * cu * cf - 3.0 * u_dot_f) + am * (3.0 * cf)))
+    return np.stack(out)
+
+
+def collide(lattice, f, wp, wm, force):
+    """TRT + Guo on every node of f (q, ...) (``collision.py:59-88``)."""
+    drho = f.sum(axis=0)
+    rho = 1.0 + drho
+    u = tuple((ja + 0.5 * fa) / rho for ja, fa in zip(_momentum(lattice, f), force, strict=True))
+    neq = f - equilibrium(lattice, drho, u)
+    neq_o = neq[list(lattice.opposite)]
+    post = f - (0.5 * wp) * (neq + neq_o) - (0.5 * wm) * (neq - neq_o)
+    if any(not _is_zero(fa) for fa in force):
+        post = post + guo_source(lattice, u, force, wp, wm)
+    return post
+
+
+def stream_pull(lattice, f):
+    """f_i(x) = f*_i(x - c_i), periodic (``streaming.py:32-37``)."""
+    axes = tuple(range(lattice.d))
+    return np.stack([np.roll(f[i], tuple(reversed(ci)), axis=axes) for i, ci in enumerate(lattice.c)])
+
+
+def bounce_back_links(lattice, solid, wall, dtype):
+    """Fluid-to-solid link mask and Ladd term 6 w_i (c_i . u_w) (``boundaries.py:53-72``)."""
+    fluid = ~solid
+    axes = tuple(range(lattice.d))
+    masks, terms = [], []
+    for ci, wi in zip(lattice.c, lattice.w, strict=True):
+        shift = tuple(reversed(ci))
+        from_solid = np.roll(solid, shift, axis=axes) & fluid
+        cu = sum(ca * np.roll(wall[a].astype(dtype), shift, axis=axes) for a, ca in enumerate(ci) if ca)
+        term = (2.0 * wi / lattice.cs2) * cu
+        masks.append(from_solid)
+        terms.append(np.where(from_solid, term, 0.0).astype(dtype))
+    return np.stack(masks), np.stack(terms)
+
+
+def _neighbour(nodes, c, shape):
+    coords = np.unravel_index(np.asarray(nodes, dtype=np.int64), shape)
+    moved = tuple((coords[a] + int(s)) % shape[a] for a, s in enumerate(tuple(c)[::-1]))
+    return np.ravel_multi_index(moved, shape)
+
+
+def _roma(r):
+    a = np.abs(np.asarray(r, dtype=np.float64))
+    inner = (1.0 + np.sqrt(np.maximum(1.0 - 3.0 * a * a, 0.0))) / 3.0
+    outer = (5.0 - 3.0 * a - np.sqrt(np.maximum(1.0 - 3.0 * (1.0 - a) ** 2, 0.0))) / 6.0
+    return np.where(a <= 0.5, inner, np.where(a <= 1.5, outer, 0.0))
+
+
+class _Ibm:
+    """Direct-forcing IBM state (``ibm.py:123-214``), reference layout only."""
+
+    def __init__(self, params, cdt):
+        body = params.immersed
+        lattice = params.lattice
+        shape = params.shape
+        d = lattice.d
+        base = np.floor(body.markers - 0.5).astype(np.int64)
+        offsets = np.indices((3,) * d).reshape(d, -1).T
+        pts = base[:, None, :] + offsets[None]
+        weights = np.prod(_roma(pts - body.markers[:, None, :]), axis=-1)
+        flat = np.ravel_multi_index(tuple(pts[..., a] for a in range(d))[::-1], shape)
+        nodes, inverse = np.unique(flat, return_inverse=True)
+        self.nodes = nodes
+        self.inverse = inverse.reshape(flat.shape)
+        self.weights = weights.astype(cdt)
+        self.areas = np.asarray(body.areas).astype(cdt)
+        self.iterations = int(body.iterations)
+        self.uniform = tuple(float(v) for v in params.force)
+        self.d = d
+        self.sources = np.stack([_neighbour(nodes, [-v for v in ck], shape) for ck in lattice.c])
+        self.c = np.asarray(lattice.c)
+        self.body_force = np.zeros(d)
+
+    def force_field(self, f):
+        q = self.sources.shape[0]
+        n = self.nodes.size
+        streamed = f.reshape(q, -1)[np.arange(q)[:, None], self.sources]  # (q, n)
+        drho = streamed.sum(axis=0)
+        rho = 1.0 + drho
+        j = [sum(self.c[k, a] * streamed[k] for k in range(q) if self.c[k, a]) for a in range(self.d)]
+        u_star = np.stack([(j[a] + 0.5 * self.uniform[a]) / rho for a in range(self.d)])
+        rho_marker = (self.weights * rho[self.inverse]).sum(axis=1)
+        force = np.zeros((self.d, n), dtype=u_star.dtype)
+        total = np.zeros(self.d, dtype=u_star.dtype)
+        flat_inv = self.inverse.reshape(-1)
+        for _ in range(self.iterations):
+            u = u_star + force / (2.0 * rho)
+            u_marker = (self.weights[None] * u[:, self.inverse]).sum(axis=2)
+            f_marker = 2.0 * rho_marker * (0.0 - u_marker) * self.areas
+            total = total + f_marker.sum(axis=1)
+            spread = (self.weights[None] * f_marker[:, :, None]).reshape(self.d, -1)
+            for a in range(self.d):
+                force[a] = force[a] + np.bincount(flat_inv, weights=spread[a], minlength=n)
+        self.body_force = -total
+        return force
+
+
+class OracleSolver:
+    """The reference solver's semantics on NumPy (``solver.py:61-292``).
+
+    Accepts any parameter object with the reference's ``SimulationParams``
+    attributes. ``force_field`` (optional, shape (d, *shape)) adds a per-node
+    Guo force on top of the uniform one (an extension used by the adjoint).
+    """
+
+    def __init__(self, params, force_field=None):
+        self.params = params
+        self.lattice = params.lattice
+        self.dtype = params.dtype
+        self.cdt = compute_dtype(params.dtype)
+        self.fluid = ~np.asarray(params.solid, dtype=bool)
+        self.solid = np.asarray(params.solid, dtype=bool)
+        self.mask, self.wall_term = bounce_back_links(self.lattice, self.solid, np.asarray(params.wall_velocity), self.cdt)
+        self.rates = params.relaxation_rates
+        self.time_step = 0
+        n = int(np.prod(params.shape))
+        self.n_nodes = n
+        self.rules = None
+        rules = params.link_rules
+        if rules is not None and len(rules):
+            v = rules.values
+            slots = np.asarray(v.direction) * n + np.asarray(v.node)
+            target = np.asarray(rules.direction) * n + np.asarray(rules.node)
+            self.rules = (target, slots, np.asarray(v.coeff).astype(self.cdt), np.asarray(v.constant).astype(self.cdt))
+        self.ibm = _Ibm(params, self.cdt) if params.immersed is not None else None
+        self.field = None
+        if self.ibm is not None:
+            self.field = np.zeros((self.lattice.d, *params.shape), dtype=self.cdt)
+        self.extra_force = None
+        if force_field is not None:
+            self.extra_force = np.asarray(force_field, dtype=self.cdt).reshape(self.lattice.d, *params.shape)
+        self.initialize()
+
+    # ---------------------------------------------------------------- state
+    def initialize(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0):
+        """Equilibrium at u + F/(2 rho), combined in float64, cast once (``solver.py:101-117``)."""
+        p = self.params
+        d = self.lattice.d
+        if d == 2 and np.any(np.asarray(uz) != 0):
+            raise ValueError("a 2D simulation has no z velocity; leave uz at 0")
+        comps = (ux, uy, uz)[:d]
+        rho = np.broadcast_to(np.asarray(rho, dtype=np.float64), p.shape)
+        force = self._force_components(np.float64)
+        u = [np.broadcast_to(np.asarray(ua, dtype=np.float64), p.shape) + 0.5 * fa / rho for ua, fa in zip(comps, force, strict=True)]
+        drho = np.asarray(rho - 1.0, dtype=self.cdt)
+        f = equilibrium(self.lattice, drho, tuple(np.asarray(a, dtype=self.cdt) for a in u))
+        self.f = quantize(f, self.dtype)
+        self.time_step = 0
+
+    def set_populations(self, f):
+        self.f = np.array(f, dtype=self.cdt, copy=True)
+
+    def _force_components(self, dt):
+        """Uniform force, plus the per-node extension field (not the IBM field)."""
+        force = tuple(float(v) for v in self.params.force)
+        if self.extra_force is None:
+            return force
+        return tuple(force[a] + self.extra_force[a].astype(dt) for a in range(self.lattice.d))
+
+    def collision_force(self):
+        force = self._force_components(self.cdt)
+        if self.field is None:
+            return force
+        return tuple(force[a] + self.field[a] for a in range(self.lattice.d))
+
+    # ---------------------------------------------------------------- step
+    def step(self):
+        """One step (``solver.py:257-274``): IBM field, pull, bounce-back, rules, collide."""
+        lattice = self.lattice
+        f = self.f
+        force = self._force_components(self.cdt)
+        if self.ibm is not None:
+            local = self.ibm.force_field(f)
+            self.field.reshape(lattice.d, -1)[:, self.ibm.nodes] = local
+            force = self.collision_force()
+        streamed = stream_pull(lattice, f)
+        reflected = f[list(lattice.opposite)] + self.wall_term
+        streamed = np.where(self.mask, reflected, streamed)
+        if self.rules is not None:
+            target, slots, coeff, const = self.rules
+            values = const + (coeff * f.reshape(-1)[slots]).sum(axis=1)
+            streamed.reshape(-1)[target] = values
+        post = collide(lattice, streamed, self.rates[0], self.rates[1], force)
+        self.f = quantize(np.where(self.fluid, post, f), self.dtype)
+
+    def run(self, steps, check_every=500):
+        done = 0
+        while done < steps:
+            k = min(check_every - done % check_every, steps - done)
+            for _ in range(k):
+                self.step()
+            self.time_step += k
+            done += k
+            self.check_health()
+
+    def check_health(self):
+        """NaN / rho <= 0 watchdog (``solver.py:162-172``)."""
+        drho = self.f.sum(axis=0)
+        bad_nf = ~np.isfinite(drho) & self.fluid
+        bad = bad_nf | ((drho <= -1.0) & self.fluid)
+        if not bad.any():
+            return
+        loc = tuple(int(i) for i in np.unravel_index(int(np.argmax(bad)), self.params.shape))
+        reason = "non-finite populations" if bad_nf.any() else "non-positive density"
+        raise OracleDiverged(self.time_step, loc, reason)
+
+    # ---------------------------------------------------------------- readouts
+    def populations(self):
+        return np.array(self.f, copy=True)
+
+    def macroscopic(self):
+        """rho = 1 + sum f~*, rho u = sum c f* - F/2; solid -> (1, 0) (``diagnostics.py:72-80``)."""
+        f = self.f
+        force = self.collision_force()
+        rho = 1.0 + f.sum(axis=0)
+        u = tuple((ja - 0.5 * fa) / rho for ja, fa in zip(_momentum(self.lattice, f), force, strict=True))
+        return np.where(self.solid, 1.0, rho), tuple(np.where(self.solid, 0.0, ua) for ua in u)
+
+    def evaluate_affine(self, compiled):
+        """const + sum coeff * f[slots] in the state dtype (``link_rules.py:269-272``)."""
+        slots = np.asarray(compiled.slots)
+        coeff = np.asarray(compiled.coeff).astype(self.cdt)
+        const = np.asarray(compiled.constant).astype(self.cdt)
+        return (const + (coeff * self.f.reshape(-1)[slots]).sum(axis=1)).astype(np.float64)
+
+    @property
+    def immersed_force(self):
+        if self.ibm is None:
+            raise AttributeError("this simulation has no immersed body")
+        return np.asarray(self.ibm.body_force, dtype=np.float64)

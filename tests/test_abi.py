@@ -1,0 +1,81 @@
+"""The C ABI without a GPU: build, load, exported symbols, device lattice tables."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import lbm_b200 as lbm
+from lbm_b200 import _native as N
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "lbm_b200.h"
+
+
+def declared_functions() -> list[str]:
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(lbm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    lbm.build.build()
+    lib = ctypes.CDLL(str(N.LIBRARY))
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(N.EXPORTED), "the ctypes binding must cover exactly the header"
+
+
+def test_abi_version_and_argument_checks_without_a_gpu():
+    lib = N.load()
+    assert lib.lbm_abi_version() == N.ABI_VERSION
+    # invalid descriptors are rejected before any CUDA call
+    bad = N.Grid(7, 0, 4, 4, 1, 4, 16)
+    assert lib.lbm_step_pull(ctypes.byref(bad), None, None, None, None, None, None, None) == N.LBM_ERR_INVALID
+    grid = N.Grid(N.LBM_D2Q9, N.LBM_F32, 4, 4, 1, 3, 12)  # pitch < nx
+    assert lib.lbm_unpack(ctypes.byref(grid), None, 0, None, None) == N.LBM_ERR_INVALID
+    assert lib.lbm_affine_reduce(0, None, None, None, None, None, 0, 0, 1, None, None, None, None) == N.LBM_ERR_INVALID
+
+
+@pytest.mark.skipif(shutil.which("nvcc") is None, reason="needs nvcc")
+def test_device_lattice_tables_match_python(tmp_path):
+    """The constexpr tables in csrc/lbm_common.cuh are host-callable: print them on the CPU."""
+    src = tmp_path / "tables.cu"
+    src.write_text(
+        '#include "lbm_common.cuh"\n#include <cstdio>\n'
+        "template <class L> void dump() { for (int i = 0; i < L::Q; ++i) "
+        'printf("%d %d %d %d %.17g\\n", L::cx(i), L::cy(i), L::cz(i), L::opp(i), L::w(i)); }\n'
+        "int main() { dump<lbm::D2Q9>(); dump<lbm::D3Q19>(); return 0; }\n"
+    )
+    exe = tmp_path / "tables"
+    csrc = ROOT / "high-performance-lbm-on-gpu-_b200" / "csrc"
+    subprocess.run(["nvcc", "-std=c++17", f"-I{csrc}", str(src), "-o", str(exe)], check=True, capture_output=True)
+    rows = [line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()]
+    for vs, block in ((lbm.D2Q9, rows[:9]), (lbm.D3Q19, rows[9:])):
+        c = np.array([[int(r[0]), int(r[1]), int(r[2])] for r in block])
+        np.testing.assert_array_equal(c, vs.c3)
+        assert [int(r[3]) for r in block] == list(vs.opposite)
+        np.testing.assert_array_equal([float(r[4]) for r in block], vs.w)
+
+
+def test_backend_registry_and_errors():
+    params = lbm.SimulationParams(nx=8, ny=8, tau=0.8)
+    with pytest.raises(ValueError, match="backend"):
+        lbm.make_solver(params, backend="opencl")
+    assert lbm.BACKENDS == ("cuda", "cuda-naive", "cuda-aa")
+
+
+def test_solver_without_gpu_raises_backend_unavailable():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the error raised on machines without a GPU")
+    with pytest.raises(lbm.BackendUnavailable):
+        lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, tau=0.8))

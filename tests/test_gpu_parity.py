@@ -1,0 +1,295 @@
+"""CUDA path against the oracle: the parity contract of the hot path (GPU).
+
+Mirrors the reference's GPU-equivalence tests (``tests/test_cuda_backend.py``,
+``test_geometry_link_rules.py``, ``test_ibm.py``, ``test_open_boundaries.py``):
+random initial state (rho = 1 + 0.01 N, u = 0.02 N, seed 0), 40 steps, fluid
+nodes compared. Tolerances: float64 |df| < 1e-15 and max|df|/max|f| <= 1e-14;
+float32 |df| < 1e-7 and relative <= 1e-6 -- the reference's absolute bounds and
+the relative bounds of the build target, whichever is tighter.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import OracleSolver
+from tests import cases
+from tests.helpers import NS
+
+import lbm_b200 as lbm
+
+pytestmark = pytest.mark.gpu
+
+BACKENDS = ["cuda-naive", "cuda-aa"]
+ABS = {"float64": 1e-15, "float32": 1e-7}
+REL = {"float64": 1e-14, "float32": 1e-6}
+
+
+def run_pair(params, backend, state=None, steps=cases.EQUIVALENCE_STEPS, **options):
+    ref = OracleSolver(params)
+    gpu = lbm.make_solver(params, backend=backend, **options)
+    if state is not None:
+        ref.initialize(*state)
+        gpu.initialize(*state)
+    ref.run(steps)
+    gpu.run(steps)
+    return ref, gpu
+
+
+def assert_parity(params, ref, gpu, dtype=None):
+    dtype = dtype or params.dtype
+    fluid = params.fluid
+    a, b = ref.populations()[:, fluid], gpu.populations()[:, fluid]
+    diff = np.abs(a - b).max()
+    assert diff < ABS[dtype], diff
+    assert diff <= REL[dtype] * np.abs(a).max(), diff
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+@pytest.mark.parametrize("collision", ["bgk", "trt"])
+def test_float64_matches_oracle_to_round_off(backend, d, collision):
+    p = cases.mixed(NS, "float64", collision, d)
+    ref, gpu = run_pair(p, backend, cases.random_state(p))
+    assert_parity(p, ref, gpu)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_float32_matches_oracle(backend, d):
+    p = cases.mixed(NS, "float32", "trt", d)
+    ref, gpu = run_pair(p, backend, cases.random_state(p))
+    assert_parity(p, ref, gpu)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_macroscopic_fields_match_oracle(backend, d):
+    p = cases.mixed(NS, "float64", "trt", d)
+    ref, gpu = run_pair(p, backend, cases.random_state(p))
+    rho, u = ref.macroscopic()
+    out = gpu.macroscopic()
+    np.testing.assert_allclose(out.rho, rho, rtol=0, atol=1e-14)
+    for a in range(d):
+        np.testing.assert_allclose(out.u[a], u[a], rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_closed_3d_box_with_moving_lid_conserves_mass(backend):
+    solid, wall = lbm.cavity_walls(n=14, lid_velocity=0.05, dimensions=3)
+    p = lbm.SimulationParams(nx=16, ny=16, nz=16, tau=0.7, solid=solid, wall_velocity=wall, dtype="float64")
+    s = lbm.make_solver(p, backend=backend)
+    m0 = s.macroscopic().total_mass
+    s.run(400)
+    assert s.macroscopic().total_mass == pytest.approx(m0, rel=1e-13)
+
+
+def test_aa_backend_advances_in_pairs_only():
+    s = lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, tau=0.8), backend="cuda-aa")
+    with pytest.raises(ValueError, match="multiples of 2"):
+        s.run(3)
+    s.run(4)
+    assert s.time_step == 4
+
+
+def test_aa_backend_uses_half_the_lattice_memory():
+    p = lbm.SimulationParams(nx=64, ny=32, tau=0.8)
+    naive, aa = lbm.make_solver(p, backend="cuda-naive"), lbm.make_solver(p, backend="cuda-aa")
+    assert aa.lattice_bytes * 2 == naive.lattice_bytes == 2 * 9 * 64 * 32 * 4
+    p3 = lbm.SimulationParams(nx=16, ny=12, nz=8, tau=0.8)
+    assert lbm.make_solver(p3, backend="cuda-aa").lattice_bytes == 19 * 16 * 12 * 8 * 4
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64", "float16", "bfloat16"])
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_kernels_keep_populations_in_registers(backend, d, dtype):
+    sizes = {"nx": 8, "ny": 8} | ({"nz": 8} if d == 3 else {})
+    s = lbm.make_solver(lbm.SimulationParams(**sizes, tau=0.8, dtype=dtype), backend=backend)
+    for name, res in s.kernel_resources().items():
+        assert res["local_bytes"] == 0, f"{name} spills to local memory"
+
+
+def test_invalid_block_is_rejected():
+    with pytest.raises(ValueError, match="block"):
+        lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, tau=0.8), backend="cuda-naive", block=(64, 32))
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_bouzidi_matches_oracle(backend, d):
+    """Every rule layout of the reference (pull, AA odd, AA even) is exercised here."""
+    for dtype in ("float64", "float32"):
+        p, _ = cases.bouzidi(NS, d, dtype)
+        ref, gpu = run_pair(p, backend, cases.random_state(p))
+        assert_parity(p, ref, gpu)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_bouzidi_with_q_one_half_equals_plain_bounce_back(backend):
+    body = lbm.circle(15.3, 10.4, 4.6)
+    solid = lbm.channel_walls(33, 21) | lbm.voxelize(body, (21, 33))
+    links = lbm.wall_links(lbm.D2Q9, body, solid)
+    half = lbm.WallLinks(links.node, links.direction, np.full(len(links), 0.5))
+    common = dict(nx=33, ny=21, tau=0.7, collision="trt", force=(1e-5, 0.0), solid=solid, dtype="float64")
+    plain = lbm.make_solver(lbm.SimulationParams(**common), backend=backend)
+    ruled = lbm.make_solver(lbm.SimulationParams(**common, link_rules=lbm.bouzidi_rules(lbm.D2Q9, half, solid)), backend=backend)
+    for s in (plain, ruled):
+        s.run(30)
+    np.testing.assert_allclose(ruled.populations(), plain.populations(), rtol=0, atol=1e-16)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_force_probe_reads_every_layout_the_same(backend, d):
+    p, links = cases.bouzidi(NS, d, "float64")
+    probe = lbm.ForceProbe.build(p, links)
+    ref, gpu = run_pair(p, backend, cases.random_state(p))
+    expect = probe.weight.T @ ref.evaluate_affine(probe.compiled("reference"))
+    np.testing.assert_allclose(probe.evaluate(gpu), expect, rtol=1e-12, atol=1e-16)
+    values = gpu.evaluate_affine(probe.compiled(gpu.state_layout))
+    np.testing.assert_allclose(probe.weight.T @ values, expect, rtol=1e-12, atol=1e-16)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_ibm_matches_oracle(backend, d):
+    for dtype, tol in (("float64", 1e-15), ("float32", 1e-7)):
+        p = cases.ibm(NS, d, dtype)
+        ref, gpu = run_pair(p, backend, cases.random_state(p))
+        assert_parity(p, ref, gpu)
+        np.testing.assert_allclose(gpu.immersed_force, ref.immersed_force, rtol=10 * tol)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_open_boundaries_match_oracle(backend, d):
+    p, _ = cases.open_channel_case(NS, d)
+    ref, gpu = run_pair(p, backend, cases.random_state(p, seed=1, u_scale=0.03))
+    assert_parity(p, ref, gpu)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_watchdog_reports_step_and_location(backend, d):
+    sizes = {"nx": 8, "ny": 8} | ({"nz": 8} if d == 3 else {})
+    s = lbm.make_solver(lbm.SimulationParams(**sizes, tau=0.8, dtype="float64"), backend=backend)
+    rho = np.ones(s.shape)
+    rho[(3, 5, 2)[:d]] = np.nan
+    s.initialize(rho)
+    with pytest.raises(lbm.SimulationDiverged) as info:
+        s.run(10, check_every=2)
+    assert info.value.step == 2
+    assert len(info.value.location) == d
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_vanishing_density_raises(backend):
+    s = lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, tau=0.8, dtype="float64"), backend=backend)
+    rho = np.ones(s.shape)
+    rho[1:4, 1:4] = -0.5
+    s.initialize(rho)
+    with pytest.raises(lbm.SimulationDiverged, match="density"):
+        s.run(2, check_every=2)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_run_counts_steps_and_fires_callback(backend):
+    s = lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, tau=0.8), backend=backend)
+    seen = []
+    s.run(12, every=4, callback=lambda sv: seen.append(sv.time_step))
+    assert s.time_step == 12 and seen == [4, 8, 12]
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_uniform_flow_is_an_exact_steady_state(backend, d):
+    velocity = (0.05, -0.02, 0.01)[:d]
+    sizes = {"nx": 8, "ny": 8} | ({"nz": 8} if d == 3 else {})
+    s = lbm.make_solver(lbm.SimulationParams(**sizes, tau=0.8, dtype="float64"), backend=backend)
+    s.initialize(1.0, *velocity)
+    s.run(50)
+    f = s.macroscopic()
+    for got, want in zip(f.u, velocity, strict=True):
+        np.testing.assert_allclose(got, want, atol=1e-14)
+    np.testing.assert_allclose(f.rho, 1.0, atol=1e-14)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_body_force_accelerates_periodic_fluid_by_f_per_step(backend, d):
+    force = (1e-5, -2e-5, 3e-5)[:d]
+    sizes = {"nx": 8, "ny": 8} | ({"nz": 8} if d == 3 else {})
+    s = lbm.make_solver(lbm.SimulationParams(**sizes, tau=0.8, dtype="float64", force=force), backend=backend)
+    s.run(40)
+    for got, fa in zip(s.macroscopic().u, force, strict=True):
+        np.testing.assert_allclose(got, 40 * fa, rtol=1e-10)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_populations_round_trip_exactly(backend):
+    p = cases.mixed(NS, "float64", "trt", 3)
+    s = lbm.make_solver(p, backend=backend)
+    s.initialize(*cases.random_state(p))
+    s.run(6)
+    f = s.populations()
+    s2 = lbm.make_solver(p, backend=backend)
+    s2.set_populations(f)
+    np.testing.assert_array_equal(s2.populations(), f)
+    s.run(6)
+    s2.run(6)
+    np.testing.assert_array_equal(s2.populations(), s.populations())
+
+
+@pytest.mark.parametrize("d", [2, 3])
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_pull_and_aa_give_identical_bits(d, dtype):
+    """Both variants compute the same per-node arithmetic on the same inputs."""
+    p, _ = cases.bouzidi(NS, d, dtype)
+    state = cases.random_state(p)
+    a = lbm.make_solver(p, backend="cuda-naive")
+    b = lbm.make_solver(p, backend="cuda-aa")
+    for s in (a, b):
+        s.initialize(*state)
+        s.run(20)
+    np.testing.assert_array_equal(a.populations()[:, p.fluid], b.populations()[:, p.fluid])
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+def test_graph_and_eager_launches_agree(backend):
+    p = cases.mixed(NS, "float32", "trt", 2)
+    a = lbm.make_solver(p, backend=backend, graph=True)
+    b = lbm.make_solver(p, backend=backend, graph=False)
+    for s in (a, b):
+        s.initialize(*cases.random_state(p))
+        s.run(70)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("pitch", [64, 96])
+def test_padded_row_pitch_changes_nothing(backend, pitch):
+    p, links = cases.bouzidi(NS, 2, "float64")
+    probe = lbm.ForceProbe.build(p, links)
+    a = lbm.make_solver(p, backend=backend)
+    b = lbm.make_solver(p, backend=backend, pitch=pitch)
+    for s in (a, b):
+        s.initialize(*cases.random_state(p))
+        s.run(10)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+    np.testing.assert_array_equal(probe.evaluate(a), probe.evaluate(b))
+
+
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("d", [2, 3])
+def test_16bit_storage_matches_emulating_oracle(backend, d, storage):
+    """The oracle rounds to the storage format like the kernels; rounding flips stay at ulp level."""
+    p = cases.mixed(NS, storage, "trt", d)
+    ref, gpu = run_pair(p, backend, cases.random_state(p), steps=10)
+    fluid = p.fluid
+    a, b = ref.populations()[:, fluid], gpu.populations()[:, fluid]
+    ulp = 2.0**-10 if storage == "float16" else 2.0**-7
+    assert np.abs(a - b).max() <= 4 * ulp * np.abs(a).max()
+    assert np.mean(a == b) > 0.95
