@@ -56,12 +56,16 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--variant", choices=("pull", "aa"), default="aa")
     ap.add_argument("--storage", choices=tuple(BYTES), default="float32")
+    ap.add_argument("--launch", choices=("split", "fused"), default="split")
+    ap.add_argument("--block", default="32x4", help="bulk tile, e.g. 32x4")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--e2e-chunk", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision-steps", type=int, default=5000,
+                    help="steps of the storage-precision study (0 = skip)")
     return ap.parse_args()
 
 
@@ -124,6 +128,7 @@ def workload_config(args):
     return {
         "workload": f"D3Q19 TRT square duct {n}x{n}x{n}, tau=0.9, Fx=1e-6, walls y/z, periodic x",
         "variant": {"pull": "two-lattice fused pull", "aa": "in-place AA pair"}[args.variant],
+        "launch": args.launch, "block": args.block,
         "storage": args.storage, "nodes": n**3, "bytes_per_update": 2 * 19 * BYTES[args.storage],
         "l2": "inputs larger than L2 (lattice %.2f GB vs 126 MB)" % (19 * n**3 * BYTES[args.storage] / 1e9),
         "parallelism": f"replicas x{args.gpus}",
@@ -212,6 +217,44 @@ def copy_peak_gbs(torch, device, nbytes=512 * 2**20, repeats=20):
     return 2 * nbytes * repeats / (a.elapsed_time(b) / 1e3) / 1e9
 
 
+def precision_study(lbm, torch, n: int, steps: int, variant: str):
+    """Duct after `steps` steps in float64, float32, float16 and bfloat16 storage.
+
+    Returns per storage: MLUPS of the run and the velocity error against the
+    float64 run (relative L2 over fluid nodes, and max |du| / max |u64|).
+    """
+    out = {}
+    ref = None
+    backend = "cuda-aa" if variant == "aa" else "cuda-naive"
+    for storage in ("float64", "float32", "float16", "bfloat16"):
+        s = lbm.make_solver(duct_params(lbm, n, storage=storage), backend=backend)
+        s._advance(2)
+        s.initialize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s._advance(steps)
+        b.record()
+        b.synchronize()
+        s.time_step = steps
+        s._check_health()
+        m = s.macroscopic()
+        u = np.stack([c.astype(np.float64) for c in m.u])
+        fluid = ~m.solid
+        entry = {"mlups": round(n**3 * steps / (a.elapsed_time(b) / 1e3) / 1e6, 1)}
+        if ref is None:
+            ref = u
+        else:
+            du = u[:, fluid] - ref[:, fluid]
+            entry["u_rel_l2_vs_f64"] = float(np.linalg.norm(du) / np.linalg.norm(ref[:, fluid]))
+            entry["u_rel_max_vs_f64"] = float(np.abs(du).max() / np.abs(ref[:, fluid]).max())
+        out[storage] = entry
+        del s
+        torch.cuda.empty_cache()
+    out["steps"] = steps
+    out["u_max_f64"] = float(np.abs(ref[0]).max())
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -224,7 +267,8 @@ def run_ours(args, rank, world, local_rank):
     nodes = n**3
     params = duct_params(lbm, n, storage=args.storage)
     backend = "cuda-aa" if args.variant == "aa" else "cuda-naive"
-    solver = lbm.make_solver(params, backend=backend)
+    block = tuple(int(v) for v in args.block.split("x"))
+    solver = lbm.make_solver(params, backend=backend, launch=args.launch, block=block)
     steps = args.steps + (args.steps % solver.step_multiple)
     warm = max(args.warmup, 3)
     warm += warm % solver.step_multiple
@@ -312,6 +356,15 @@ def run_ours(args, rank, world, local_rank):
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if args.precision_steps > 0 and world == 1:
+        del solver
+        torch.cuda.empty_cache()
+        study = precision_study(lbm, torch, n, args.precision_steps, args.variant)
+        line["storage_precision"] = study
+        fp16 = study["float16"]
+        line["fp16_store"] = {"mlups": fp16["mlups"], "vs_fp32_mlups": round(fp16["mlups"] / study["float32"]["mlups"], 3),
+                              "u_rel_l2_vs_f64": fp16["u_rel_l2_vs_f64"], "u_rel_max_vs_f64": fp16["u_rel_max_vs_f64"],
+                              "steps": args.precision_steps}
     if not args.no_cpu_baseline and world == 1:
         mlups_cpu, done, dt = oracle_mlups(n, 8, 3, 1, budget=args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(mlups_cpu, 4), "unit": "MLUPS", "cores": 1, "kind": "port",

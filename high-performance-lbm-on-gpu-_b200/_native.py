@@ -18,7 +18,8 @@ LBM_D2Q9, LBM_D3Q19 = 0, 1
 LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
 LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
 LAYOUT_PULL, LAYOUT_AA_ODD, LAYOUT_AA_EVEN = 0, 1, 2
-KIND_SOLID, KIND_SPECIAL, KIND_NEAR = 1, 2, 4
+KIND_SOLID, KIND_SPECIAL, KIND_NEAR, KIND_EDGE = 1, 2, 4, 8
+LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY = 0, 1, 2
 
 STORAGE_CODE = {"float32": LBM_F32, "float64": LBM_F64, "float16": LBM_F16, "bfloat16": LBM_BF16}
 LATTICE_CODE = {"D2Q9": LBM_D2Q9, "D3Q19": LBM_D3Q19}
@@ -56,7 +57,7 @@ class Special(C.Structure):
 
 
 class Launch(C.Structure):
-    _fields_ = [("tile_x", i32), ("tile_y", i32)]
+    _fields_ = [("tile_x", i32), ("tile_y", i32), ("mode", i32)]
 
 
 class Ibm(C.Structure):
@@ -67,8 +68,35 @@ class Ibm(C.Structure):
     ]
 
 
+class Adjoint(C.Structure):
+    _fields_ = [
+        ("gather_start", vp), ("gather_dir", vp), ("gather_slot", vp), ("gather_coeff", vp), ("rule_dconst", vp),
+        ("term_dcoeff", vp), ("rule_du", vp), ("force_grad", vp),
+    ]
+
+
+class Domain(C.Structure):
+    _fields_ = [
+        ("nx", i32), ("ny", i32), ("nz", i32), ("pitch", i32), ("offset", i64), ("qstride", i64),
+        ("kind_offset", i64), ("wall_offset", i64), ("omega_plus", C.c_double), ("omega_minus", C.c_double),
+        ("force", C.c_double * 3),
+    ]
+
+
+class Batch(C.Structure):
+    _fields_ = [
+        ("lattice", i32), ("storage", i32), ("n_domains", i32), ("domains", vp), ("n_tiles", i32), ("tiles", vp),
+        ("n_boundary", i32), ("boundary_domain", vp), ("boundary_node", vp), ("tile_x", i32), ("tile_y", i32),
+        ("blocks", i32), ("kind", vp), ("wall_u", vp),
+    ]
+
+
 P = C.POINTER
 _SIGNATURES = {
+    "lbm_adjoint_step": [P(Grid), P(Physics), P(Special), P(Adjoint), P(Launch), vp, vp, vp, vp, C.c_double, vp],
+    "lbm_adjoint_initial": [P(Grid), P(Physics), P(Special), P(Adjoint), vp, vp, vp, vp, C.c_double, vp],
+    "lbm_batch_step": [P(Batch), vp, vp, vp],
+    "lbm_batch_occupancy": [i32, i32, i32, i32, vp],
     "lbm_step_pull": [P(Grid), P(Physics), P(Special), P(Launch), vp, vp, vp, vp],
     "lbm_step_aa": [P(Grid), P(Physics), P(Special), P(Launch), vp, vp, i32, vp],
     "lbm_export_prime": [P(Grid), P(Special), vp, i32, vp, vp],

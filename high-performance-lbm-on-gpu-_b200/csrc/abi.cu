@@ -38,22 +38,18 @@ static bool special_valid(const lbm_special_t* sp, bool aa)
 }
 
 static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
-                     const lbm_launch_t* launch, const uint8_t* kind, const void* src, void* dst, int& threads)
+                     const lbm_launch_t* launch, const uint8_t* kind, const void* src, void* dst, int& tx, int& ty,
+                     int& mode)
 {
-    const int tx = launch ? launch->tile_x : 32;
-    const int ty = launch ? launch->tile_y : 8;
+    tx = launch ? launch->tile_x : 32;
+    ty = launch ? launch->tile_y : 4;
+    mode = launch ? launch->mode : LBM_LAUNCH_FUSED;
     if (tx <= 0 || ty <= 0 || tx % 32 != 0 || tx * ty > 256) return LBM_ERR_INVALID;
-    threads = tx * ty;
     a.nx = g->nx;
     a.ny = g->ny;
     a.nz = g->nz;
     a.pitch = g->pitch;
     a.qstride = g->qstride;
-    a.tile_x = tx;
-    a.tile_y = ty;
-    a.tiles_x = (g->nx + tx - 1) / tx;
-    a.tiles_y = (g->ny + ty - 1) / ty;
-    a.bulk_blocks = (int64_t)a.tiles_x * a.tiles_y * g->nz;
     a.wp = p->omega_plus;
     a.wm = p->omega_minus;
     a.fx = p->force[0];
@@ -72,9 +68,9 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
 }
 
 template <class L, int ST>
-static int step_dispatch(const StepArgs& a, int variant, int threads, cudaStream_t s)
+static int step_dispatch(const StepArgs& a, int variant, int mode, int tx, int ty, cudaStream_t s)
 {
-    return launch_step<L, ST>(a, variant, threads, s);
+    return launch_step<L, ST>(a, variant, mode, tx, ty, s);
 }
 
 extern "C" int lbm_step_pull(const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
@@ -84,11 +80,11 @@ extern "C" int lbm_step_pull(const lbm_grid_t* g, const lbm_physics_t* p, const 
     if (!grid_valid(g) || !p || !kind || !f_src || !f_dst || f_src == f_dst || !special_valid(sp, false))
         return LBM_ERR_INVALID;
     StepArgs a;
-    int threads = 0;
-    int st = make_args(a, g, p, sp, launch, kind, f_src, f_dst, threads);
+    int tx = 0, ty = 0, mode = 0;
+    int st = make_args(a, g, p, sp, launch, kind, f_src, f_dst, tx, ty, mode);
     if (st != LBM_OK) return st;
     const int lattice = g->lattice, storage = g->storage;
-    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, LBM_PULL, threads, (cudaStream_t)stream); };
+    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, LBM_PULL, mode, tx, ty, (cudaStream_t)stream); };
     return record(run());
 }
 
@@ -99,11 +95,11 @@ extern "C" int lbm_step_aa(const lbm_grid_t* g, const lbm_physics_t* p, const lb
     if (!grid_valid(g) || !p || !kind || !f || !special_valid(sp, true)) return LBM_ERR_INVALID;
     if (parity != LBM_AA_EVEN && parity != LBM_AA_ODD) return LBM_ERR_INVALID;
     StepArgs a;
-    int threads = 0;
-    int st = make_args(a, g, p, sp, launch, kind, f, f, threads);
+    int tx = 0, ty = 0, mode = 0;
+    int st = make_args(a, g, p, sp, launch, kind, f, f, tx, ty, mode);
     if (st != LBM_OK) return st;
     const int lattice = g->lattice, storage = g->storage;
-    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, parity, threads, (cudaStream_t)stream); };
+    auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, parity, mode, tx, ty, (cudaStream_t)stream); };
     return record(run());
 }
 

@@ -122,7 +122,8 @@ __global__ void classify_kernel(const lbm_grid_t g, const uint8_t* __restrict__ 
         const int sz = L::D == 3 ? wrap(z - L::cz(i), g.nz) : 0;
         near |= solid[((int64_t)sz * g.ny + sy) * g.pitch + sx] != 0;
     }
-    kind[nd] = near ? KIND_NEAR : KIND_FLUID;
+    const bool edge = x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1 || (L::D == 3 && (z == 0 || z == g.nz - 1));
+    kind[nd] = (near ? KIND_NEAR : KIND_FLUID) | (edge ? KIND_EDGE : KIND_FLUID);
 }
 
 __global__ void mark_special_kernel(const int64_t* __restrict__ nodes, int n, uint8_t* kind)

@@ -5,7 +5,7 @@
 
 namespace lbm {
 
-template <class L, int ST> int launch_step(const StepArgs& a, int variant, int threads, cudaStream_t stream);
+template <class L, int ST> int launch_step(const StepArgs& a, int variant, int mode, int tile_x, int tile_y, cudaStream_t stream);
 template <class L, int ST> int step_resources(int variant, int32_t* out4);
 
 // Invoke FN<L, ST>(args...) for the run-time lattice and storage codes.

@@ -20,11 +20,14 @@ namespace lbm {
 // link rules, an immersed-boundary force or rule-term exports and are updated
 // by the boundary warps from a compact list; the bulk threads skip them.
 // NEAR marks fluid nodes with at least one solid neighbour: only they test
-// their neighbours' kinds, every other node streams without a branch.
+// their neighbours' kinds. EDGE marks fluid nodes on a face of the box, whose
+// neighbours wrap periodically. A node with kind 0 is interior: it streams
+// with fixed, warp-uniform offsets and no branch at all.
 constexpr uint8_t KIND_FLUID = 0;
 constexpr uint8_t KIND_SOLID = LBM_KIND_SOLID;
 constexpr uint8_t KIND_SPECIAL = LBM_KIND_SPECIAL;
 constexpr uint8_t KIND_NEAR = LBM_KIND_NEAR;
+constexpr uint8_t KIND_EDGE = LBM_KIND_EDGE;
 
 // ---------------------------------------------------------------- lattices
 // Tables are constexpr functions of a direction index: every direction loop
@@ -112,13 +115,19 @@ template <> struct Storage<LBM_BF16> {
 
 // ---------------------------------------------------------------- collision
 // TRT + Guo forcing on one node (reference src/lbm/collision.py:59-88,
-// forcing.py:37-56), written over opposite pairs (i, o) as even/odd parts:
-//   f+ = (f_i + f_o)/2, f- = (f_i - f_o)/2
-//   feq+ = w (drho + rho (4.5 cu^2 - 1.5 u.u)), feq- = 3 w rho cu
-//   S+ = w (1 - w+/2)(9 cu cF - 3 u.F),        S- = 3 w (1 - w-/2) cF
+// forcing.py:37-56). With rho = 1 + sum f~, u = (sum c f + F/2)/rho and, for
+// each opposite pair (i, o = opp i), cu = c_i.u and cF = c_i.F, the update
 //   f*_i = f_i - w+ (f+ - feq+) - w- (f- - feq-) + S+ + S-
-//   f*_o = f_o - w+ (f+ - feq+) + w- (f- - feq-) + S+ - S-
-// with rho = 1 + sum f~ and u = (sum c f + F/2)/rho. BGK is w- = w+.
+// (f+- = (f_i +- f_o)/2, feq+ = w (drho + rho (4.5 cu^2 - 1.5 u.u)),
+//  feq- = 3 w rho cu, S+ = w (1 - w+/2)(9 cu cF - 3 u.F), S- = 3 w (1 - w-/2) cF)
+// is evaluated in factored form
+//   f*_i = a f_i + b f_o + E + O,   f*_o = a f_o + b f_i + E - O
+//   a = 1 - (w+ + w-)/2,  b = (w- - w+)/2
+//   E = w (A + cu (B cu + C cF)),  O = w (D cu + G cF)
+//   A = w+ (drho - 1.5 rho u.u) - 3 (1 - w+/2) u.F,  B = 4.5 w+ rho,  C = 9 (1 - w+/2)
+//   D = 3 w- rho,  G = 3 (1 - w-/2)
+// so each pair costs ~15 operations; the node-level scalars are shared. BGK
+// is w- = w+ (b = 0). The rest population: f*_0 = (1 - w+) f_0 + w_0 A.
 template <class L, class R>
 __device__ __forceinline__ void collide(R (&f)[L::Q], R wp, R wm, R Fx, R Fy, R Fz)
 {
@@ -134,18 +143,22 @@ __device__ __forceinline__ void collide(R (&f)[L::Q], R wp, R wm, R Fx, R Fy, R 
         if (L::cz(i) < 0) jz -= f[i];
     }
     const R rho = R(1) + drho;
-    const R ux = (jx + R(0.5) * Fx) / rho;
-    const R uy = (jy + R(0.5) * Fy) / rho;
-    const R uz = L::D == 3 ? (jz + R(0.5) * Fz) / rho : R(0);
-    const R usq = R(1.5) * (ux * ux + uy * uy + uz * uz);
+    const R inv = R(1) / rho;
+    const R ux = (jx + R(0.5) * Fx) * inv;
+    const R uy = (jy + R(0.5) * Fy) * inv;
+    const R uz = L::D == 3 ? (jz + R(0.5) * Fz) * inv : R(0);
+    const R usq = ux * ux + uy * uy + uz * uz;
     const R uF = ux * Fx + uy * Fy + (L::D == 3 ? uz * Fz : R(0));
     const R ap = R(1) - R(0.5) * wp;
     const R am = R(1) - R(0.5) * wm;
-    {
-        const R w0 = R(L::w(0));
-        const R feq = w0 * (drho - rho * usq);
-        f[0] = f[0] - wp * (f[0] - feq) + w0 * ap * (R(-3) * uF);
-    }
+    const R A = wp * (drho - R(1.5) * rho * usq) - R(3) * ap * uF;
+    const R B = R(4.5) * wp * rho;
+    const R C = R(9) * ap;
+    const R Dm = R(3) * wm * rho;
+    const R G = R(3) * am;
+    const R ca = R(1) - R(0.5) * (wp + wm);
+    const R cb = R(0.5) * (wm - wp);
+    f[0] = (R(1) - wp) * f[0] + R(L::w(0)) * A;
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
         const int o = L::opp(i);
@@ -153,15 +166,11 @@ __device__ __forceinline__ void collide(R (&f)[L::Q], R wp, R wm, R Fx, R Fy, R 
         const R wi = R(L::w(i));
         const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
         const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
-        const R feq_even = wi * (drho + rho * (R(4.5) * cu * cu - usq));
-        const R feq_odd = wi * rho * (R(3) * cu);
-        const R dp = wp * (R(0.5) * (f[i] + f[o]) - feq_even);
-        const R dm = wm * (R(0.5) * (f[i] - f[o]) - feq_odd);
-        const R sp = wi * ap * (R(9) * cu * cF - R(3) * uF);
-        const R sm = wi * am * (R(3) * cF);
+        const R E = wi * (A + cu * (B * cu + C * cF));
+        const R O = wi * (Dm * cu + G * cF);
         const R fi = f[i], fo = f[o];
-        f[i] = fi - dp - dm + sp + sm;
-        f[o] = fo - dp + dm + sp - sm;
+        f[i] = ca * fi + (cb * fo + (E + O));
+        f[o] = ca * fo + (cb * fi + (E - O));
     }
 }
 
@@ -185,8 +194,6 @@ __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >=
 struct StepArgs {
     int nx, ny, nz, pitch;
     int64_t qstride;  // elements between direction planes (pitch * ny * nz)
-    int tile_x, tile_y, tiles_x, tiles_y;
-    int64_t bulk_blocks;
     double wp, wm, fx, fy, fz;
     const uint8_t* kind;
     const void* f_src;

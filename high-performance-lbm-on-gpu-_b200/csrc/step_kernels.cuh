@@ -3,13 +3,15 @@
 //
 // One launch updates every fluid node once:
 //   * bulk blocks: a (tile_x x tile_y) tile of one z plane, one node per
-//     thread. A thread reads its kind byte; SOLID and SPECIAL nodes return,
-//     NEAR nodes test the kind of each source (bounce-back), every other node
-//     streams with no branch at all.
-//   * boundary warps: the blocks after the bulk range walk the compact list
-//     of SPECIAL nodes (link rules, immersed-boundary force, AA rule-term
-//     exports). They run the same per-node code with the rule and force
-//     look-ups switched on, so rules need no separate pre-pass launch.
+//     thread. Interior nodes (kind 0) stream with fixed, warp-uniform
+//     offsets and no branch; every other node returns.
+//   * boundary warps: one thread per entry of the compact list of all other
+//     fluid nodes -- next to a wall (bounce-back, Ladd term), on a periodic
+//     face (wrap), carrying link rules, an immersed-boundary force or AA
+//     rule-term exports. Rules are evaluated in registers while the node
+//     is updated, so they need no pre-pass launch and no scatter.
+//   The boundary warps run in the same launch (FUSED) or as a second kernel
+//   that may overlap the bulk (BULK + BOUNDARY); see lbm_launch_t.
 //
 // Race freedom.
 //   Pull: f_src is never written; rules read it directly.
@@ -52,6 +54,49 @@ struct StepKernel {
             for (int t = sp.term_start[r]; t < t1; ++t) v += coeff[t] * ex[sp.term_export[t]];
         }
         return v;
+    }
+
+    // Interior fluid node (kind 0: no solid neighbour, not on a face of the
+    // box, no rule or local force). Every source and destination offset is
+    // the same for all threads (-c_i . strides), so the compiler keeps them in
+    // uniform registers and each access is [thread pointer + uniform offset].
+    // All Q loads are independent and issued back to back.
+    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd)
+    {
+        const int64_t qs = a.qstride;
+        const int64_t py = a.pitch;
+        const int64_t pz = (int64_t)a.pitch * a.ny;
+        R f[Q];
+        const T* fs = static_cast<const T*>(a.f_src) + nd;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int64_t shift = L::cx(i) + L::cy(i) * py + L::cz(i) * pz;
+            if (VAR == LBM_AA_EVEN)
+                f[i] = S::load(fs + i * qs);
+            else if (VAR == LBM_PULL)
+                f[i] = S::load_nc(fs + (i * qs - shift));
+            else
+                f[i] = S::load(fs + (L::opp(i) * qs - shift));
+        }
+        R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
+        if (a.force_field != nullptr) {
+            const R* ff = static_cast<const R*>(a.force_field);
+            Fx += ff[nd];
+            Fy += ff[qs + nd];
+            if (L::D == 3) Fz += ff[2 * qs + nd];
+        }
+        collide<L, R>(f, R(a.wp), R(a.wm), Fx, Fy, Fz);
+        T* fd = static_cast<T*>(a.f_dst) + nd;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int64_t shift = L::cx(i) + L::cy(i) * py + L::cz(i) * pz;
+            if (VAR == LBM_PULL)
+                S::store(fd + i * qs, f[i]);
+            else if (VAR == LBM_AA_EVEN)
+                S::store(fd + L::opp(i) * qs, f[i]);
+            else
+                S::store(fd + (i * qs + shift), f[i]);
+        }
     }
 
     template <bool SPECIAL>
@@ -175,64 +220,116 @@ struct StepKernel {
     }
 };
 
+// Bulk: interior nodes (kind 0) of tile (blockIdx.x, blockIdx.y) of plane
+// blockIdx.z. Every other non-solid node is in the special list.
 template <class L, int ST, int VAR>
-__global__ void __launch_bounds__(256) lbm_step_kernel(const StepArgs a)
+__device__ __forceinline__ void bulk_tile(const StepArgs& a, int z)
 {
-    using K = StepKernel<L, ST, VAR>;
-    const int64_t b = blockIdx.x;
-    if (b < a.bulk_blocks) {
-        const int tx = threadIdx.x % a.tile_x;
-        const int ty = threadIdx.x / a.tile_x;
-        int64_t t = b;
-        const int bx = (int)(t % a.tiles_x);
-        t /= a.tiles_x;
-        const int by = (int)(t % a.tiles_y);
-        const int z = (int)(t / a.tiles_y);
-        const int x = bx * a.tile_x + tx;
-        const int y = by * a.tile_y + ty;
-        if (x >= a.nx || y >= a.ny) return;
-        const int64_t nd = ((int64_t)z * a.ny + y) * a.pitch + x;
-        const uint8_t k = a.kind[nd];
-        if (k & (KIND_SOLID | KIND_SPECIAL)) return;
-        K::template node<false>(a, x, y, z, nd, (k & KIND_NEAR) != 0, -1);
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.nx || y >= a.ny) return;
+    const int64_t nd = ((int64_t)z * a.ny + y) * a.pitch + x;
+    if (a.kind[nd] == KIND_FLUID) StepKernel<L, ST, VAR>::interior(a, nd);
+}
+
+template <class L, int ST, int VAR>
+__device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
+{
+    if (s >= a.sp.n_special) return;
+    const int64_t nd = a.sp.node[s];
+    const int64_t row = nd / a.pitch;
+    const int x = (int)(nd - row * a.pitch);
+    const int y = (int)(row % a.ny);
+    const int z = (int)(row / a.ny);
+    StepKernel<L, ST, VAR>::template node<true>(a, x, y, z, nd, (a.kind[nd] & KIND_NEAR) != 0, s);
+}
+
+// FUSED: grid (ceil(nx/bx), ceil(ny/by), nz + extra); planes z >= nz are
+// boundary warps. BULK: the same grid without the extra planes.
+// Bulk-only launches: ptxas's default register target (no spills, high
+// occupancy) -- this kernel carries almost all of the traffic.
+template <class L, int ST, int VAR>
+__global__ void __launch_bounds__(256) lbm_bulk_kernel(const StepArgs a)
+{
+    bulk_tile<L, ST, VAR>(a, blockIdx.z);
+}
+
+// FUSED: grid (ceil(nx/bx), ceil(ny/by), nz + extra), planes z >= nz are
+// boundary warps. BOUNDARY: 1D grid over the list. Up to 255 registers, so
+// the general per-node path never spills.
+template <class L, int ST, int VAR, int MODE>
+__global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
+{
+    if (MODE == LBM_LAUNCH_BOUNDARY) {
+        boundary_node<L, ST, VAR>(a, blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+        return;
+    }
+    const int z = blockIdx.z;
+    if (z < a.nz) {
+        bulk_tile<L, ST, VAR>(a, z);
     } else {
-        const int64_t s = (b - a.bulk_blocks) * (int64_t)blockDim.x + threadIdx.x;
-        if (s >= a.sp.n_special) return;
-        const int64_t nd = a.sp.node[s];
-        const int64_t row = nd / a.pitch;
-        const int x = (int)(nd - row * a.pitch);
-        const int y = (int)(row % a.ny);
-        const int z = (int)(row / a.ny);
-        K::template node<true>(a, x, y, z, nd, (a.kind[nd] & KIND_NEAR) != 0, s);
+        const int64_t b = ((int64_t)(z - a.nz) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        boundary_node<L, ST, VAR>(a, b * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x);
     }
 }
 
-template <class L, int ST>
-int launch_step(const StepArgs& a, int variant, int threads, cudaStream_t stream)
+template <class L, int ST, int VAR>
+static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cudaStream_t stream)
 {
-    const int64_t special_blocks = (a.sp.n_special + threads - 1) / threads;
-    const int64_t blocks = a.bulk_blocks + special_blocks;
-    if (blocks <= 0) return LBM_OK;
-    if (blocks > 0x7fffffffLL) return LBM_ERR_INVALID;
-    switch (variant) {
-    case LBM_PULL: lbm_step_kernel<L, ST, LBM_PULL><<<(unsigned)blocks, threads, 0, stream>>>(a); break;
-    case LBM_AA_EVEN: lbm_step_kernel<L, ST, LBM_AA_EVEN><<<(unsigned)blocks, threads, 0, stream>>>(a); break;
-    case LBM_AA_ODD: lbm_step_kernel<L, ST, LBM_AA_ODD><<<(unsigned)blocks, threads, 0, stream>>>(a); break;
-    default: return LBM_ERR_INVALID;
+    const int threads = tile_x * tile_y;
+    const unsigned gx = (unsigned)((a.nx + tile_x - 1) / tile_x);
+    const unsigned gy = (unsigned)((a.ny + tile_y - 1) / tile_y);
+    if (mode == LBM_LAUNCH_BOUNDARY) {
+        if (a.sp.n_special <= 0) return LBM_OK;
+        const int64_t blocks = (a.sp.n_special + 255) / 256;
+        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY><<<(unsigned)blocks, 256, 0, stream>>>(a);
+    } else if (mode == LBM_LAUNCH_BULK) {
+        if (a.nz > 65535) return LBM_ERR_INVALID;
+        lbm_bulk_kernel<L, ST, VAR><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+    } else {
+        const int64_t per_plane = (int64_t)gx * gy * threads;
+        const int64_t extra = a.sp.n_special > 0 ? (a.sp.n_special + per_plane - 1) / per_plane : 0;
+        if (a.nz + extra > 65535) return LBM_ERR_INVALID;
+        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED>
+            <<<dim3(gx, gy, (unsigned)(a.nz + extra)), dim3(tile_x, tile_y), 0, stream>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
 }
 
 template <class L, int ST>
-int step_resources(int variant, int32_t* out4)
+int launch_step(const StepArgs& a, int variant, int mode, int tile_x, int tile_y, cudaStream_t stream)
+{
+    if (mode < LBM_LAUNCH_FUSED || mode > LBM_LAUNCH_BOUNDARY) return LBM_ERR_INVALID;
+    switch (variant) {
+    case LBM_PULL: return launch_mode<L, ST, LBM_PULL>(a, mode, tile_x, tile_y, stream);
+    case LBM_AA_EVEN: return launch_mode<L, ST, LBM_AA_EVEN>(a, mode, tile_x, tile_y, stream);
+    case LBM_AA_ODD: return launch_mode<L, ST, LBM_AA_ODD>(a, mode, tile_x, tile_y, stream);
+    default: return LBM_ERR_INVALID;
+    }
+}
+
+template <class L, int ST, int VAR>
+static cudaError_t attrs(cudaFuncAttributes* attr, int mode)
+{
+    switch (mode) {
+    case LBM_LAUNCH_FUSED: return cudaFuncGetAttributes(attr, lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED>);
+    case LBM_LAUNCH_BULK: return cudaFuncGetAttributes(attr, lbm_bulk_kernel<L, ST, VAR>);
+    default: return cudaFuncGetAttributes(attr, lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY>);
+    }
+}
+
+// which = variant + 3 * mode
+template <class L, int ST>
+int step_resources(int which, int32_t* out4)
 {
     cudaFuncAttributes attr;
     cudaError_t e;
+    const int variant = which % 3, mode = which / 3;
+    if (mode > LBM_LAUNCH_BOUNDARY || which < 0) return LBM_ERR_INVALID;
     switch (variant) {
-    case LBM_PULL: e = cudaFuncGetAttributes(&attr, lbm_step_kernel<L, ST, LBM_PULL>); break;
-    case LBM_AA_EVEN: e = cudaFuncGetAttributes(&attr, lbm_step_kernel<L, ST, LBM_AA_EVEN>); break;
-    case LBM_AA_ODD: e = cudaFuncGetAttributes(&attr, lbm_step_kernel<L, ST, LBM_AA_ODD>); break;
-    default: return LBM_ERR_INVALID;
+    case LBM_PULL: e = attrs<L, ST, LBM_PULL>(&attr, mode); break;
+    case LBM_AA_EVEN: e = attrs<L, ST, LBM_AA_EVEN>(&attr, mode); break;
+    default: e = attrs<L, ST, LBM_AA_ODD>(&attr, mode); break;
     }
     if (e != cudaSuccess) return LBM_ERR_LAUNCH;
     out4[0] = attr.numRegs;
@@ -245,5 +342,5 @@ int step_resources(int variant, int32_t* out4)
 }  // namespace lbm
 
 #define LBM_INSTANTIATE_STEP(L, ST)                                                        \
-    template int lbm::launch_step<lbm::L, ST>(const lbm::StepArgs&, int, int, cudaStream_t); \
+    template int lbm::launch_step<lbm::L, ST>(const lbm::StepArgs&, int, int, int, int, cudaStream_t); \
     template int lbm::step_resources<lbm::L, ST>(int, int32_t*);

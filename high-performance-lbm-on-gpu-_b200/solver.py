@@ -32,7 +32,7 @@ from .lattice import as_lattice
 from .params import COMPUTE_DTYPE
 
 DEFAULT_CHECK_EVERY = 500
-DEFAULT_BLOCK = (32, 8)
+DEFAULT_BLOCK = (32, 4)
 BACKENDS = ("cuda", "cuda-naive", "cuda-aa")
 VARIANTS = ("pull", "aa")
 
@@ -164,9 +164,12 @@ class CudaSolver(Solver):
     """
 
     def __init__(self, params, variant: str = "pull", block=DEFAULT_BLOCK, force_field=None,
-                 graph: bool = True, device=None, pitch: int | None = None):
+                 graph: bool = True, device=None, pitch: int | None = None, launch: str = "split",
+                 keep_zero_terms: bool = False):
         if variant not in VARIANTS:
             raise ValueError(f"unknown CUDA variant {variant!r}; choose from {VARIANTS}")
+        if launch not in ("fused", "split"):
+            raise ValueError(f"launch must be 'fused' or 'split'; got {launch!r}")
         bx, by = (int(b) for b in block)
         if bx <= 0 or by <= 0 or bx * by > 1024:
             raise ValueError(f"block must be positive with at most 1024 threads; got {block}")
@@ -209,7 +212,9 @@ class CudaSolver(Solver):
         self.t_store = tdt[self.storage]
         self.t_real = tdt[self.compute]
         self.grid = N.Grid(N.LATTICE_CODE[lattice.name], N.STORAGE_CODE[self.storage], nx, ny, nz, self.pitch, self.qstride)
-        self.launch = N.Launch(bx, by)
+        self.launch_mode = launch
+        self.keep_zero_terms = bool(keep_zero_terms)
+        self._launches = {m: N.Launch(bx, by, m) for m in (N.LAUNCH_FUSED, N.LAUNCH_BULK, N.LAUNCH_BOUNDARY)}
         self.block = (bx, by)
 
         # ---- physics
@@ -230,15 +235,8 @@ class CudaSolver(Solver):
             if force_field is not None:
                 raise ValueError("a per-node force field cannot be combined with an immersed body")
             self._ibm = _IbmState(self, build_tables(params.immersed, lattice, np.asarray(params.solid)))
-        self._special = self._build_special(params)
-
-        # ---- node kinds
-        solid = self._upload_scalar(np.asarray(params.solid, dtype=np.uint8), torch.uint8)
-        self._kind = torch.empty(self.qstride, dtype=torch.uint8, device=self.device)
-        sp_nodes = self._special.tensors.get("node")
-        self._native("lbm_classify", N.C.byref(self.grid), N.ptr(solid), N.ptr(sp_nodes), self._special.n_special,
-                     N.ptr(self._kind), self._stream())
         self._solid_host = np.asarray(params.solid, dtype=bool)
+        self._special = self._build_special(params)
 
         # ---- populations
         self._f = torch.empty((q, self.qstride), dtype=self.t_store, device=self.device)
@@ -282,13 +280,20 @@ class CudaSolver(Solver):
 
     # ------------------------------------------------------------------ special nodes
     def _build_special(self, params) -> _SpecialTables:
+        """Classify the nodes on the device and build the boundary-warp list.
+
+        The list holds every fluid node that is not interior: next to a wall,
+        on a periodic face, carrying link rules, an immersed-boundary force or
+        (AA) rule-term exports. Rules are sorted by (node, direction).
+        """
         torch = self.torch
         lat = self.lattice
         n = self.n_nodes
         rules = params.link_rules
-        rule_nodes = np.zeros(0, dtype=np.int64)
         t = {}
         n_rules = n_terms = n_export = 0
+        rule_nodes = np.zeros(0, dtype=np.int64)
+        rule_dir = np.zeros(0, dtype=np.int64)
         if rules is not None and len(rules):
             node = np.asarray(rules.node, dtype=np.int64)
             direction = np.asarray(rules.direction, dtype=np.int64)
@@ -300,45 +305,54 @@ class CudaSolver(Solver):
             order = np.lexsort((direction, node))
             node, direction = node[order], direction[order]
             coeff, tdir, tnode, const = coeff[order], tdir[order], tnode[order], const[order]
-            live = coeff != 0.0
-            counts = live.sum(axis=1)
+            # keep_zero_terms: a fixed term structure (the adjoint aligns derivatives with it)
+            live = np.ones_like(coeff, dtype=bool) if self.keep_zero_terms else coeff != 0.0
+            self._rule_order, self._rule_live = order, live
             start = np.zeros(len(node) + 1, dtype=np.int64)
-            np.cumsum(counts, out=start[1:])
-            term_dir = tdir[live]
-            term_node = tnode[live]
-            term_coeff = coeff[live]
+            np.cumsum(live.sum(axis=1), out=start[1:])
+            term_dir, term_node, term_coeff = tdir[live], tnode[live], coeff[live]
             n_rules, n_terms = len(node), int(start[-1])
             if n_terms >= 2**31:
                 raise ValueError("too many rule terms")
             if np.any(term_node < 0) or np.any(term_node >= n) or np.any(term_dir < 0) or np.any(term_dir >= lat.q):
                 raise ValueError("a rule term points outside the lattice")
-            rule_nodes = node
+            rule_nodes, rule_dir = self._pitched(node), direction
             t["term_start"] = torch.from_numpy(start.astype(np.int32)).to(self.device)
             t["rule_const"] = torch.from_numpy(const).to(self.device, self.t_real)
             t["term_dir"] = torch.from_numpy(term_dir.astype(np.int32)).to(self.device)
             t["term_node"] = torch.from_numpy(self._pitched(term_node)).to(self.device)
             t["term_coeff"] = torch.from_numpy(term_coeff).to(self.device, self.t_real)
-            rule_dir = direction
-        ibm_nodes = self._ibm.tables.nodes if self._ibm is not None else np.zeros(0, dtype=np.int64)
-        export_nodes = np.zeros(0, dtype=np.int64)
+        ibm_nodes = self._pitched(self._ibm.tables.nodes) if self._ibm is not None else np.zeros(0, dtype=np.int64)
+        export_nodes = export_dirs = np.zeros(0, dtype=np.int64)
         if self.variant == "aa" and n_rules:
-            solid = np.asarray(params.solid, dtype=bool).ravel()
-            if np.any(solid[term_node]):
+            if np.any(self._solid_host.ravel()[term_node]):
                 raise ValueError("the AA variant needs every rule term on a fluid node")
-            keys = term_node * 32 + term_dir
+            keys = self._pitched(term_node) * 32 + term_dir
             ukeys, term_export = np.unique(keys, return_inverse=True)
             n_export = ukeys.size
-            export_nodes = ukeys // 32
-            export_dirs = ukeys % 32
+            export_nodes, export_dirs = ukeys // 32, ukeys % 32
             t["term_export"] = torch.from_numpy(term_export.astype(np.int32)).to(self.device)
-        nodes = np.unique(np.concatenate([rule_nodes, ibm_nodes, export_nodes]))
+            t["export_a"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
+            t["export_b"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
+
+        # ---- node kinds on the device; marked nodes get the SPECIAL bit
+        marked = np.unique(np.concatenate([rule_nodes, ibm_nodes, export_nodes]))
+        marked_t = torch.from_numpy(marked).to(self.device) if marked.size else None
+        solid = self._upload_scalar(self._solid_host.astype(np.uint8), torch.uint8)
+        self._kind = torch.empty(self.qstride, dtype=torch.uint8, device=self.device)
+        self._native("lbm_classify", N.C.byref(self.grid), N.ptr(solid), N.ptr(marked_t), int(marked.size),
+                     N.ptr(self._kind), self._stream())
+        k = self._kind
+        listed = torch.nonzero((k != 0) & ((k & N.KIND_SOLID) == 0)).flatten()
+        nodes = listed.cpu().numpy().astype(np.int64)  # ascending pitched indices
         ns = nodes.size
         if ns == 0:
             return _SpecialTables({}, 0, 0, 0, 0, 0)
+        if ns >= 2**31:
+            raise ValueError("too many boundary nodes")
         rule_mask = np.zeros(ns, dtype=np.uint32)
         rule_first = np.zeros(ns, dtype=np.int32)
         if n_rules:
-            # rules are sorted by (node, direction): a node's rules start at its first occurrence
             pos = np.searchsorted(nodes, rule_nodes)
             np.bitwise_or.at(rule_mask, pos, (np.uint32(1) << rule_dir.astype(np.uint32)))
             rule_first = np.searchsorted(rule_nodes, nodes, side="left").astype(np.int32)
@@ -350,11 +364,8 @@ class CudaSolver(Solver):
         if n_export:
             pos = np.searchsorted(nodes, export_nodes)
             np.bitwise_or.at(export_mask, pos, (np.uint32(1) << export_dirs.astype(np.uint32)))
-            # exports are sorted by (node, direction) through their keys
             export_first = np.searchsorted(export_nodes, nodes, side="left").astype(np.int32)
-            t["export_a"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
-            t["export_b"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
-        t["node"] = torch.from_numpy(self._pitched(nodes)).to(self.device)
+        t["node"] = listed.contiguous()
         t["rule_mask"] = torch.from_numpy(rule_mask.view(np.int32)).to(self.device)
         t["rule_first"] = torch.from_numpy(rule_first).to(self.device)
         t["force_slot"] = torch.from_numpy(force_slot).to(self.device)
@@ -476,12 +487,39 @@ class CudaSolver(Solver):
         return self._f
 
     # ------------------------------------------------------------------ stepping
+    def _step_launch(self, name, sp, *tail):
+        """One time step: a fused launch, or bulk + boundary kernels forked onto two streams."""
+        g, ph = N.C.byref(self.grid), N.C.byref(self.physics)
+        if self.launch_mode == "fused" or self._special.n_special == 0:
+            mode = N.LAUNCH_FUSED if self._special.n_special else N.LAUNCH_BULK
+            self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[mode]), N.ptr(self._kind), *tail,
+                         self._stream())
+            return
+        torch = self.torch
+        main = torch.cuda.current_stream(self.device)
+        side = self._side_stream
+        fork, join = torch.cuda.Event(), torch.cuda.Event()
+        fork.record(main)
+        side.wait_event(fork)
+        self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[N.LAUNCH_BOUNDARY]), N.ptr(self._kind), *tail,
+                     side.cuda_stream)
+        join.record(side)
+        self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[N.LAUNCH_BULK]), N.ptr(self._kind), *tail,
+                     main.cuda_stream)
+        main.wait_event(join)
+
+    @property
+    def _side_stream(self):
+        s = getattr(self, "_side", None)
+        if s is None:
+            s = self._side = self.torch.cuda.Stream(self.device)
+        return s
+
     def _launch_pull(self):
         if self._ibm is not None:
             self._ibm.run(self._f, N.LAYOUT_PULL)
         sp = self._special_struct()
-        self._native("lbm_step_pull", N.C.byref(self.grid), N.C.byref(self.physics), N.C.byref(sp), N.C.byref(self.launch),
-                     N.ptr(self._kind), N.ptr(self._f), N.ptr(self._f_next), self._stream())
+        self._step_launch("lbm_step_pull", sp, N.ptr(self._f), N.ptr(self._f_next))
         self._f, self._f_next = self._f_next, self._f
 
     def _launch_aa(self, parity, layout):
@@ -491,8 +529,7 @@ class CudaSolver(Solver):
         if self._special.n_export:
             ex_in, ex_out = self._export_cur, self._export_nxt
         sp = self._special_struct(ex_in, ex_out)
-        self._native("lbm_step_aa", N.C.byref(self.grid), N.C.byref(self.physics), N.C.byref(sp), N.C.byref(self.launch),
-                     N.ptr(self._kind), N.ptr(self._f), parity, self._stream())
+        self._step_launch("lbm_step_aa", sp, N.ptr(self._f), parity)
         if self._special.n_export:
             self._export_cur, self._export_nxt = self._export_nxt, self._export_cur
 
@@ -628,12 +665,16 @@ class CudaSolver(Solver):
     def kernel_resources(self) -> dict[str, dict[str, int]]:
         """Registers, spill bytes and shared memory of the step kernels (``cuda_solver.py:311-326``)."""
         lib = N.load()
-        which = {"aa_odd": N.LBM_AA_ODD, "aa_even": N.LBM_AA_EVEN} if self.variant == "aa" else {"stream_collide_pull": N.LBM_PULL}
+        variants = {"aa_odd": N.LBM_AA_ODD, "aa_even": N.LBM_AA_EVEN} if self.variant == "aa" else {"pull": N.LBM_PULL}
+        modes = {"fused": N.LAUNCH_FUSED} if self.launch_mode == "fused" else {"bulk": N.LAUNCH_BULK, "boundary": N.LAUNCH_BOUNDARY}
         out = {}
-        for name, code in which.items():
-            buf = (N.i32 * 4)()
-            N.check(lib.lbm_kernel_resources(self.grid.lattice, self.grid.storage, code, buf), "lbm_kernel_resources")
-            out[name] = {"registers": buf[0], "local_bytes": buf[1], "shared_bytes": buf[2], "max_threads": buf[3]}
+        for vname, code in variants.items():
+            for mname, mode in modes.items():
+                buf = (N.i32 * 4)()
+                N.check(lib.lbm_kernel_resources(self.grid.lattice, self.grid.storage, code + 3 * mode, buf),
+                        "lbm_kernel_resources")
+                out[f"{vname}_{mname}"] = {"registers": buf[0], "local_bytes": buf[1], "shared_bytes": buf[2],
+                                           "max_threads": buf[3]}
         return out
 
 

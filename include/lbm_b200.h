@@ -38,8 +38,10 @@ enum { LBM_F32 = 0, LBM_F64 = 1, LBM_F16 = 2, LBM_BF16 = 3 };
 enum { LBM_PULL = 0, LBM_AA_EVEN = 1, LBM_AA_ODD = 2 };
 /* Where a stored state keeps f*_k(y) (reference src/lbm/link_rules.py:16-25). */
 enum { LBM_LAYOUT_PULL = 0, LBM_LAYOUT_AA_ODD = 1, LBM_LAYOUT_AA_EVEN = 2 };
-/* Node kind bits (one byte per node). */
-enum { LBM_KIND_SOLID = 1, LBM_KIND_SPECIAL = 2, LBM_KIND_NEAR = 4 };
+/* Node kind bits (one byte per node): SOLID; SPECIAL (updated by the boundary
+ * warps); NEAR (fluid with a solid neighbour); EDGE (fluid on a face of the
+ * box, neighbours wrap periodically). Kind 0 = interior fluid node. */
+enum { LBM_KIND_SOLID = 1, LBM_KIND_SPECIAL = 2, LBM_KIND_NEAR = 4, LBM_KIND_EDGE = 8 };
 
 /* ---- descriptors ------------------------------------------------------ */
 typedef struct lbm_grid {
@@ -87,10 +89,22 @@ typedef struct lbm_special {
     void* export_out;             /* AA: real[n_export] read by the next launch */
 } lbm_special_t;
 
-/* Bulk tiling of a step launch: tile_x * tile_y threads per block, one node each. */
+/* How a step is launched. The bulk grid covers the interior fluid nodes
+ * (kind 0) with blocks of tile_x * tile_y threads, one node each, over
+ * (ceil(nx/tile_x), ceil(ny/tile_y), nz). Every other fluid node (near a
+ * wall, on a periodic face, with rules, an immersed-boundary force or
+ * exports) must be in the special list and is updated by the boundary warps:
+ *   LBM_LAUNCH_FUSED    one launch, boundary warps in extra z-planes of blocks;
+ *   LBM_LAUNCH_BULK     the bulk grid only;
+ *   LBM_LAUNCH_BOUNDARY the boundary warps only (1D grid over the list).
+ * BULK and BOUNDARY touch disjoint nodes and may run concurrently; together
+ * they are one time step. Split launches let the bulk kernel keep its small
+ * register budget. */
+enum { LBM_LAUNCH_FUSED = 0, LBM_LAUNCH_BULK = 1, LBM_LAUNCH_BOUNDARY = 2 };
 typedef struct lbm_launch {
     int32_t tile_x;   /* multiple of 32 */
-    int32_t tile_y;
+    int32_t tile_y;   /* tile_x * tile_y <= 256 */
+    int32_t mode;     /* LBM_LAUNCH_* */
 } lbm_launch_t;
 
 /* ---- the time step ---------------------------------------------------- */
@@ -120,7 +134,7 @@ int lbm_export_prime(const lbm_grid_t* grid, const lbm_special_t* sp, const void
 
 /* ---- node kinds -------------------------------------------------------- */
 
-/* kind[node] = SOLID | SPECIAL | NEAR from a solid mask (uint8, 0/1, pitched
+/* kind[node] = SOLID | SPECIAL | NEAR | EDGE from a solid mask (uint8, 0/1, pitched
  * like the lattice) and a list of special nodes. Periodic neighbours. */
 int lbm_classify(const lbm_grid_t* grid, const uint8_t* solid, const int64_t* special_nodes,
                  int32_t n_special, uint8_t* kind, lbm_stream_t stream);
@@ -209,11 +223,92 @@ int lbm_ibm_iteration(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iter
 int lbm_ibm_body_force(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iterations, double* out,
                        lbm_stream_t stream);
 
+/* ---- adjoint (reverse mode) of the two-lattice step ---------------------- */
+
+/* Extra tables of the adjoint step, per node of the adjoint special list (the
+ * forward list plus every node that a rule term or the loss reads).
+ *   gather[g] for g in [gather_start[s], gather_start[s+1]): direction k of
+ *   the node and a contribution coeff * mu[slot] (slot >= 0) or coeff * loss_scale
+ *   (slot < 0, the loss gradient of a force probe) to lambda_k(node). */
+typedef struct lbm_adjoint {
+    const int32_t* gather_start;   /* n_special + 1 */
+    const int32_t* gather_dir;
+    const int64_t* gather_slot;    /* slot of mu (k * qstride + pitched node) or -1 */
+    const void* gather_coeff;      /* real */
+    const void* rule_dconst;       /* real[n_rules]: d const / dU of each rule, or NULL */
+    const void* term_dcoeff;       /* real[n_terms]: d coeff / dU aligned with the rule terms */
+    double* rule_du;               /* double[n_rules] accumulator: sum over steps of mu_j * d rule value / dU */
+    void* force_grad;              /* real[d][qstride] accumulator of dL/dG, or NULL */
+} lbm_adjoint_t;
+
+/* One backward step of the two-lattice pull scheme, fused:
+ *   lambda_{t+1}(x) = reverse-pull of mu_next (bounce-back and link rules
+ *       transposed) + loss_scale * dD/df at probe slots;
+ *   s_t(x) = streamed populations of f_t (recomputed, as the forward step);
+ *   mu_t(x) = J_C(s_t(x), F(x))^T lambda_{t+1}(x)       -> mu_out
+ *   force_grad(x) += J_F^T lambda_{t+1}(x); rule_du += mu_j * d value / dU.
+ * mu_next may be NULL (lambda_T = loss_scale * dD/df). Traffic: read f_t and
+ * mu_next, write mu_out (3 Q values per node). Same launch modes as the step. */
+int lbm_adjoint_step(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm_special_t* sp,
+                     const lbm_adjoint_t* adj, const lbm_launch_t* launch, const uint8_t* kind,
+                     const void* f_t, const void* mu_next, void* mu_out, double loss_scale,
+                     lbm_stream_t stream);
+
+/* Closing term: lambda_0 = reverse-pull of mu_0, and force_grad += the
+ * derivative of the initial equilibrium (velocity shifted by F/(2 rho), F
+ * including the per-node force) w.r.t. the per-node force. rho0/u0: the
+ * float64 fields the state was initialised from (pitched). */
+int lbm_adjoint_initial(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm_special_t* sp,
+                        const lbm_adjoint_t* adj, const uint8_t* kind, const void* mu0, const double* rho0,
+                        const double* u0, double loss_scale, lbm_stream_t stream);
+
+/* ---- batched domains (many independent lattices, one launch per step) ---- */
+
+/* One domain of a batch: a lattice of its own in pooled buffers. */
+typedef struct lbm_domain {
+    int32_t nx, ny, nz, pitch;
+    int64_t offset;        /* element offset of the domain's direction-0 plane in the population pools */
+    int64_t qstride;       /* pitch * ny * nz */
+    int64_t kind_offset;   /* byte offset of the domain's kind array in the kind pool */
+    int64_t wall_offset;   /* element offset of its wall velocity (d planes of qstride) or -1 */
+    double omega_plus, omega_minus;
+    double force[3];
+} lbm_domain_t;
+
+/* Work list of a batch step: n_tiles bulk tiles, each int32 x4 = (domain,
+ * tile index along x, tile index along y, z), then the boundary list (every
+ * non-interior fluid node of every domain) in chunks of tile_x * tile_y.
+ * A persistent grid of `blocks` blocks walks the items round-robin; no block
+ * waits for another. */
+typedef struct lbm_batch {
+    int32_t lattice, storage;
+    int32_t n_domains;
+    const lbm_domain_t* domains;   /* device array */
+    int32_t n_tiles;
+    const int32_t* tiles;          /* device, 4 int32 per tile */
+    int32_t n_boundary;
+    const int32_t* boundary_domain;  /* device */
+    const int64_t* boundary_node;    /* device, pitched node index inside the domain */
+    int32_t tile_x, tile_y;        /* tile_x multiple of 32, tile_x * tile_y <= 256 */
+    int32_t blocks;                /* persistent grid size (> 0) */
+    const uint8_t* kind;           /* kind pool */
+    const void* wall_u;            /* wall pool (compute type) or NULL */
+} lbm_batch_t;
+
+/* One two-lattice pull step of every domain of the batch -- the batched
+ * counterpart of lbm_step_pull (no link rules or immersed bodies). */
+int lbm_batch_step(const lbm_batch_t* batch, const void* f_src, void* f_dst, lbm_stream_t stream);
+
+/* Blocks of the batch kernel that fit on one SM for the given tile (occupancy
+ * API), for sizing the persistent grid. */
+int lbm_batch_occupancy(int32_t lattice, int32_t storage, int32_t tile_x, int32_t tile_y, int32_t* blocks_per_sm);
+
 /* ---- diagnostics ------------------------------------------------------- */
 
 /* Registers, local (spill) bytes, static shared bytes and max threads per
  * block of one step kernel; replaces CudaSolver.kernel_resources
- * (cuda_solver.py:311-326). which = LBM_PULL / LBM_AA_EVEN / LBM_AA_ODD. */
+ * (cuda_solver.py:311-326). which = variant + 3 * launch mode
+ * (variant LBM_PULL / LBM_AA_EVEN / LBM_AA_ODD, mode LBM_LAUNCH_*). */
 int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t which, int32_t* out4);
 
 /* Name of the last CUDA error seen by the library in this thread (static string). */

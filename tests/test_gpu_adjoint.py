@@ -1,0 +1,149 @@
+"""Hand-written adjoint against the FP64 NumPy adjoint and finite differences (GPU).
+
+The loss is the momentum-exchange drag on a Bouzidi body averaged over the
+last steps of a run from rest; the parameters are the Zou-He inlet-speed
+scale U and a per-node Guo force field G. The NumPy adjoint
+(``oracle/adjoint.py``) differentiates the oracle by complex steps and an
+explicit transposed-streaming scatter, independently of the CUDA kernels.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.adjoint import OracleAdjoint
+
+import lbm_b200 as lbm
+from lbm_b200.adjoint import AdjointRun, aligned_rules, drag_loss
+
+pytestmark = pytest.mark.gpu
+
+
+def channel_2d(dtype="float64"):
+    lat = lbm.D2Q9
+    nx, ny = 24, 14
+    solid = lbm.channel_walls(nx, ny)
+    body = lbm.circle(9.3, 6.6, 2.7)
+    solid |= lbm.voxelize(body, solid.shape)
+    inflow = np.zeros((2, ny))
+    inflow[0, 1:-1] = 0.04
+
+    def make(scale):
+        s2, rules, d_rules = lbm.zou_he_inlet_derivative(lat, solid, scale * inflow)
+        links = lbm.wall_links(lat, body, s2)
+        all_rules, all_d = aligned_rules(rules, d_rules, lbm.bouzidi_rules(lat, links, s2))
+        p = lbm.SimulationParams(nx=nx, ny=ny, tau=0.6, collision="trt", solid=s2, dtype=dtype, link_rules=all_rules)
+        return p, all_d
+
+    p, _ = make(1.0)
+    links = lbm.wall_links(lat, body, p.solid)
+    return make, links, p
+
+
+def channel_3d(dtype="float64"):
+    lat = lbm.D3Q19
+    nx, ny, nz = 20, 12, 11
+    solid = lbm.duct_walls(nx, ny, nz)
+    body = lbm.sphere(7.2, 5.6, 5.3, 2.3)
+    solid |= lbm.voxelize(body, solid.shape)
+    inflow = np.zeros((3, nz, ny))
+    inflow[0, 1:-1, 1:-1] = 0.04
+
+    def make(scale):
+        s2, rules, d_rules = lbm.zou_he_inlet_derivative(lat, solid, scale * inflow)
+        links = lbm.wall_links(lat, body, s2)
+        all_rules, all_d = aligned_rules(rules, d_rules, lbm.bouzidi_rules(lat, links, s2))
+        p = lbm.SimulationParams(nx=nx, ny=ny, nz=nz, tau=0.6, collision="trt", solid=s2, dtype=dtype,
+                                 link_rules=all_rules)
+        return p, all_d
+
+    p, _ = make(1.0)
+    links = lbm.wall_links(lat, body, p.solid)
+    return make, links, p
+
+
+def oracle_gradients(make, links, G, steps, window):
+    p, d_rules = make(1.0)
+    probe = lbm.ForceProbe.build(p, links)
+    comp = probe.compiled("reference")
+    adj = OracleAdjoint(p, (comp.slots, comp.coeff, comp.constant), probe.weight, 0, window, G, d_rules)
+    loss = adj.forward(steps)
+    dU, dG = adj.backward()
+    return loss, dU, dG
+
+
+@pytest.mark.parametrize("case", [channel_2d, channel_3d], ids=["2d", "3d"])
+def test_adjoint_matches_the_numpy_adjoint_in_float64(case):
+    make, links, p = case("float64")
+    rng = np.random.default_rng(0)
+    G = 1e-5 * rng.standard_normal((p.d, *p.shape)) * p.fluid
+    steps, window = 30, 12
+    loss_ref, dU_ref, dG_ref = oracle_gradients(make, links, G, steps, window)
+    run = AdjointRun(make, links, steps=steps, window=window, checkpoint=7)
+    loss = run.forward(1.0, G)
+    dU, dG = run.backward()
+    assert loss == pytest.approx(loss_ref, rel=1e-12)
+    assert dU == pytest.approx(dU_ref, rel=1e-10)
+    fluid = p.fluid
+    np.testing.assert_allclose(dG[:, fluid], dG_ref[:, fluid], rtol=0, atol=1e-10 * np.abs(dG_ref).max())
+
+
+def test_adjoint_matches_central_finite_differences():
+    """Central differences with h = 1e-4 relative, float64 runs (agreement <= 1e-4)."""
+    make, links, p = channel_2d("float64")
+    rng = np.random.default_rng(1)
+    G = 1e-5 * rng.standard_normal((p.d, *p.shape)) * p.fluid
+    steps, window = 40, 15
+    run = AdjointRun(make, links, steps=steps, window=window, checkpoint=10)
+    run.forward(1.0, G)
+    dU, dG = run.backward()
+    h = 1e-4
+    fd_U = (run.forward(1.0 + h, G) - run.forward(1.0 - h, G)) / (2 * h)
+    assert abs(dU - fd_U) <= 1e-4 * abs(fd_U)
+    v = rng.standard_normal(G.shape) * p.fluid
+    eps = 1e-4 * np.abs(G).max()
+    fd_G = (run.forward(1.0, G + eps * v) - run.forward(1.0, G - eps * v)) / (2 * eps)
+    assert abs((dG * v).sum() - fd_G) <= 1e-4 * abs(fd_G)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    make, links, p = channel_2d("float64")
+    G = np.zeros((p.d, *p.shape))
+    out = []
+    for k in (1, 8, 1000):
+        run = AdjointRun(make, links, steps=24, window=10, checkpoint=k)
+        run.forward(1.0, G)
+        out.append(run.backward())
+    for dU, dG in out[1:]:
+        assert dU == out[0][0]
+        np.testing.assert_array_equal(dG, out[0][1])
+
+
+def test_float32_adjoint_is_close_to_the_float64_adjoint():
+    make64, links, p = channel_2d("float64")
+    make32, _, _ = channel_2d("float32")
+    rng = np.random.default_rng(2)
+    G = 1e-5 * rng.standard_normal((p.d, *p.shape)) * p.fluid
+    a = AdjointRun(make64, links, steps=40, window=15)
+    b = AdjointRun(make32, links, steps=40, window=15)
+    a.forward(1.0, G)
+    b.forward(1.0, G)
+    dU64, dG64 = a.backward()
+    dU32, dG32 = b.backward()
+    assert dU32 == pytest.approx(dU64, rel=1e-4)
+    assert np.abs(dG32 - dG64).max() <= 1e-4 * np.abs(dG64).max()
+
+
+def test_torch_autograd_function():
+    import torch
+
+    make, links, p = channel_2d("float64")
+    run = AdjointRun(make, links, steps=20, window=8)
+    U = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    G = torch.zeros((p.d, *p.shape), dtype=torch.float64, requires_grad=True)
+    loss = drag_loss(U, G, run)
+    loss.backward()
+    dU, dG = run.backward()
+    assert U.grad.item() == pytest.approx(dU, rel=1e-14)
+    np.testing.assert_allclose(G.grad.numpy(), dG, rtol=1e-14)

@@ -1,0 +1,138 @@
+"""The benchmark configurations at their own sizes (GPU).
+
+Oracle parity where the oracle finishes in seconds (few steps at full size,
+or full length on a reduced grid); size-independent properties elsewhere:
+analytic decay, pull == AA bit equality, mass conservation, steady profiles.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import OracleSolver
+from tests import cases
+from tests.helpers import NS
+
+import lbm_b200 as lbm
+
+pytestmark = pytest.mark.gpu
+
+
+# ---------------------------------------------------------------- D2Q9 Taylor-Green 512^2
+def test_taylor_green_512_matches_oracle_and_decays_at_the_lattice_viscosity():
+    p, state = cases.tgv(NS, n=512)
+    gpu = lbm.make_solver(p, backend="cuda-naive")
+    gpu.initialize(*state)
+    ref = OracleSolver(p)
+    ref.initialize(*state)
+    gpu.run(100)
+    ref.run(100)
+    fluid = p.fluid
+    a, b = ref.populations(), gpu.populations()
+    assert np.abs(a - b).max() < 1e-7
+    # velocity amplitude decays as exp(-2 nu k^2 t), nu = (tau - 1/2)/3
+    gpu.run(900)
+    f = gpu.macroscopic()
+    k = 2 * math.pi / 512
+    nu = (0.8 - 0.5) / 3
+    y, x = np.mgrid[0:512, 0:512]
+    shape_x = 0.01 * np.sin(k * x) * np.cos(k * y)
+    amp = float((f.ux * shape_x).sum() / (shape_x * shape_x).sum())
+    assert amp / 0.01 == pytest.approx(math.exp(-2 * nu * k * k * 1000), rel=2e-4)
+    assert fluid.all()
+
+
+# ---------------------------------------------------------------- D3Q19 duct 256^3
+@pytest.mark.parametrize("storage", ["float32", "float16", "bfloat16"])
+def test_duct_256_pull_and_aa_agree_bit_for_bit(storage):
+    p = cases.duct(NS, n=256, dtype=storage)
+    a = lbm.make_solver(p, backend="cuda-naive")
+    b = lbm.make_solver(p, backend="cuda-aa")
+    for s in (a, b):
+        s.run(40)
+    fa, fb = a.populations(), b.populations()
+    fluid = p.fluid
+    assert np.array_equal(fa[:, fluid], fb[:, fluid])
+
+
+def test_duct_128_matches_oracle_for_two_steps():
+    """The oracle's NumPy temporaries at 256^3 would need ~15 GB of host memory; 128^3 keeps it near 2 GB."""
+    p = cases.duct(NS, n=128, dtype="float32")
+    ref = OracleSolver(p)
+    gpu = lbm.make_solver(p, backend="cuda-aa")
+    ref.run(2)
+    gpu.run(2)
+    assert np.abs(ref.populations() - gpu.populations()).max() < 1e-9
+
+
+def test_duct_reduced_full_length_matches_oracle():
+    """The duct cross-section at 4 x 34 x 34 for the configuration's 5000 steps."""
+    p = cases.duct(NS, n=34, nx=4, dtype="float32")
+    ref = OracleSolver(p)
+    gpu = lbm.make_solver(p, backend="cuda-aa")
+    ref.run(5000)
+    gpu.run(5000)
+    fluid = p.fluid
+    a, b = ref.populations()[:, fluid], gpu.populations()[:, fluid]
+    assert np.abs(a - b).max() <= 1e-6 * np.abs(a).max()
+
+
+def test_duct_steady_profile_matches_the_fourier_series():
+    """H = 16 square duct run to steady state: L2 error < 1e-3 (reference test_duct_flow.py:67-69)."""
+    h = 16
+    nu = (0.9 - 0.5) / 3
+    y = np.arange(1, h + 1) - 0.5
+    n = (2 * np.arange(2000) + 1).astype(np.float64)[:, None, None]
+    yy, zz = y[None, None, :], y[None, :, None]
+    a_ = n * math.pi * np.abs(zz - 0.5 * h) / h
+    b_ = n * math.pi * 0.5
+    ratio = np.exp(a_ - b_) * (1 + np.exp(-2 * a_)) / (1 + np.exp(-2 * b_))
+    shape = 4 * h * h / (nu * math.pi**3) * (np.sin(n * math.pi * yy / h) * (1 - ratio) / n**3).sum(axis=0)
+    force = 0.01 / shape.max()
+    p = cases.duct(NS, n=h + 2, nx=4, dtype="float32", force=force)
+    s = lbm.make_solver(p, backend="cuda-aa")
+    s.run(20000)
+    u = s.macroscopic().ux[1:-1, 1:-1, :].mean(axis=-1)
+    exact = force * shape
+    assert np.linalg.norm(u - exact) / np.linalg.norm(exact) < 1e-3
+
+
+def test_duct_256_float64_conserves_mass():
+    p = cases.duct(NS, n=128, dtype="float64")
+    s = lbm.make_solver(p, backend="cuda-naive")
+    m0 = s.macroscopic().total_mass
+    s.run(200)
+    assert s.macroscopic().total_mass == pytest.approx(m0, rel=1e-13)
+
+
+# ---------------------------------------------------------------- D2Q9 cylinder channel
+@pytest.mark.parametrize("method", ["bouzidi", "ibm"])
+def test_cylinder_channel_matches_oracle(method):
+    p, _, _ = cases.cylinder_channel(NS, method, dtype="float32")
+    ref = OracleSolver(p)
+    gpu = lbm.make_solver(p, backend="cuda-naive")
+    ref.run(30)
+    gpu.run(30)
+    fluid = p.fluid
+    a, b = ref.populations()[:, fluid], gpu.populations()[:, fluid]
+    assert np.abs(a - b).max() < 1e-7
+    if method == "ibm":
+        np.testing.assert_allclose(gpu.immersed_force, ref.immersed_force, rtol=1e-5, atol=1e-9)
+
+
+# ---------------------------------------------------------------- batched cavities
+def test_batched_cavity_config_domains_match_single_runs():
+    from lbm_b200.batched import BatchedSolver, cavity_batch
+
+    params, sizes, _ = cavity_batch(lbm, count=256, seed=0)
+    chosen = [0, 17, 255]
+    batch = BatchedSolver(params, block=(32, 4))
+    batch.run(100)
+    for i in chosen:
+        alone = lbm.make_solver(params[i], backend="cuda-naive")
+        alone.run(100)
+        np.testing.assert_array_equal(batch.populations(i), alone.populations())
+    assert batch.nodes == int(((sizes + 2) ** 2).sum())
