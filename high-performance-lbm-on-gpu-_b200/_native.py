@@ -20,6 +20,7 @@ LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
 LAYOUT_PULL, LAYOUT_AA_ODD, LAYOUT_AA_EVEN = 0, 1, 2
 KIND_SOLID, KIND_SPECIAL, KIND_NEAR, KIND_EDGE = 1, 2, 4, 8
 LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY = 0, 1, 2
+LAUNCH_MODES = (LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY)
 
 STORAGE_CODE = {"float32": LBM_F32, "float64": LBM_F64, "float16": LBM_F16, "bfloat16": LBM_BF16}
 LATTICE_CODE = {"D2Q9": LBM_D2Q9, "D3Q19": LBM_D3Q19}
@@ -43,7 +44,7 @@ class Grid(C.Structure):
 class Physics(C.Structure):
     _fields_ = [
         ("omega_plus", C.c_double), ("omega_minus", C.c_double), ("force", C.c_double * 3),
-        ("wall_u", vp), ("force_field", vp),
+        ("wall_u", vp), ("force_field", vp), ("solid_nbr", vp),
     ]
 
 
@@ -86,8 +87,7 @@ class Domain(C.Structure):
 class Batch(C.Structure):
     _fields_ = [
         ("lattice", i32), ("storage", i32), ("n_domains", i32), ("domains", vp), ("n_tiles", i32), ("tiles", vp),
-        ("n_boundary", i32), ("boundary_domain", vp), ("boundary_node", vp), ("tile_x", i32), ("tile_y", i32),
-        ("blocks", i32), ("kind", vp), ("wall_u", vp),
+        ("tile_x", i32), ("tile_y", i32), ("blocks", i32), ("kind", vp), ("solid_nbr", vp), ("wall_u", vp),
     ]
 
 
@@ -100,7 +100,7 @@ _SIGNATURES = {
     "lbm_step_pull": [P(Grid), P(Physics), P(Special), P(Launch), vp, vp, vp, vp],
     "lbm_step_aa": [P(Grid), P(Physics), P(Special), P(Launch), vp, vp, i32, vp],
     "lbm_export_prime": [P(Grid), P(Special), vp, i32, vp, vp],
-    "lbm_classify": [P(Grid), vp, vp, i32, vp, vp],
+    "lbm_classify": [P(Grid), vp, vp, i32, vp, vp, vp],
     "lbm_init_equilibrium": [P(Grid), P(Physics), vp, vp, i32, vp, vp],
     "lbm_unpack": [P(Grid), vp, i32, vp, vp],
     "lbm_pack": [P(Grid), vp, i32, vp, vp],

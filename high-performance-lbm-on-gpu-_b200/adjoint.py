@@ -85,7 +85,11 @@ class AdjointRun:
         self._build_adjoint_tables(comp, probe.weight[:, self.axis])
 
     def _build_adjoint_tables(self, comp, w_axis):
-        """Adjoint special list: forward list + rule-term nodes + probe nodes, with gather tables."""
+        """Adjoint special list: forward special nodes + rule-term nodes + probe nodes, with gather tables.
+
+        Nodes only next to a wall or on a periodic face stay with the bulk
+        adjoint kernel (solid-neighbour masks from the forward classification).
+        """
         s = self.solver
         torch = s.torch
         lat = s.lattice
@@ -146,6 +150,7 @@ class AdjointRun:
         # kind: adjoint-list nodes are SPECIAL so the bulk skips them
         self._adj_kind = s._kind.clone()
         self._adj_kind[self._adj_t["node"]] |= N.KIND_SPECIAL
+
         # rule derivative tables (aligned with the device rule terms)
         self._rule_du = None
         if self.d_rules is not None and s._special.n_rules:

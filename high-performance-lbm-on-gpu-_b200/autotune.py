@@ -69,7 +69,7 @@ def tune_step(solver, tiles=TILES, steps: int = 20) -> dict:
         results = {}
         steps += steps % solver.step_multiple
         for tx, ty in tiles:
-            solver._launches = {m: N.Launch(tx, ty, m) for m in (N.LAUNCH_FUSED, N.LAUNCH_BULK, N.LAUNCH_BOUNDARY)}
+            solver._launches = {m: N.Launch(tx, ty, m) for m in N.LAUNCH_MODES}
             solver._graphs.clear()
             results[f"{tx}x{ty}"] = _time(solver.torch, solver._advance, steps)
         best = min(results, key=results.get)
@@ -77,7 +77,7 @@ def tune_step(solver, tiles=TILES, steps: int = 20) -> dict:
         _store()
     best = _CACHE[key]
     tx, ty = best["block"]
-    solver._launches = {m: N.Launch(tx, ty, m) for m in (N.LAUNCH_FUSED, N.LAUNCH_BULK, N.LAUNCH_BOUNDARY)}
+    solver._launches = {m: N.Launch(tx, ty, m) for m in N.LAUNCH_MODES}
     solver.block = (tx, ty)
     solver._graphs.clear()
     return best

@@ -1,11 +1,11 @@
 """Many independent domains of uneven size, one persistent launch per step.
 
-``BatchedSolver`` packs every domain's populations, node kinds and wall
-velocities into pooled device buffers, builds one work list (bulk tiles of all
-domains, then the cross-domain list of non-interior fluid nodes) and advances
-all of them with ``lbm_batch_step`` -- a persistent kernel whose blocks walk
-the list round-robin without waiting for each other (``csrc/batch.cu``). Steps
-are replayed from CUDA graphs. Tile shape and grid size come from
+``BatchedSolver`` packs every domain's populations, node kinds,
+solid-neighbour masks and wall velocities into pooled device buffers, builds
+one work list of tiles over all domains and advances all of them with
+``lbm_batch_step`` -- a persistent kernel whose blocks walk the list
+round-robin without waiting for each other (``csrc/batch.cu``). Steps are
+replayed from CUDA graphs. Tile shape and grid size come from
 ``autotune.tune_batch`` unless given.
 
 The reference has no batched mode; each domain evolves exactly as the same
@@ -108,20 +108,16 @@ class BatchedSolver:
                 self._wall[w0 : w0 + d * g.qstride].view(d, g.qstride)[:, :n] = torch.from_numpy(
                     np.ascontiguousarray(wall)).to(self.device, self.t_real)
 
-        # ---- node kinds and the boundary list, domain by domain
+        # ---- node kinds and solid-neighbour masks, domain by domain
+        self._nbr = torch.zeros(koff, dtype=torch.int32, device=self.device)
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        bdom, bnode = [], []
         for i, (p, g) in enumerate(zip(self.params, self.grids, strict=True)):
+            solid = torch.zeros(g.qstride, dtype=torch.uint8, device=self.device)
             n = g.nx * g.ny * g.nz
-            solid = torch.from_numpy(np.asarray(p.solid, dtype=np.uint8).reshape(-1)).to(self.device)
-            kind = self._kind[self.kind_offsets[i] : self.kind_offsets[i] + g.qstride]
-            N.call("lbm_classify", N.C.byref(g), N.ptr(solid), None, 0, N.ptr(kind), stream)
-            k = kind[:n]
-            listed = torch.nonzero((k != 0) & ((k & N.KIND_SOLID) == 0)).flatten()
-            bnode.append(listed)
-            bdom.append(torch.full_like(listed, i, dtype=torch.int32))
-        self._bnode = torch.cat(bnode).to(torch.int64).contiguous()
-        self._bdom = torch.cat(bdom).to(torch.int32).contiguous()
+            solid[:n] = torch.from_numpy(np.asarray(p.solid, dtype=np.uint8).reshape(-1)).to(self.device)
+            k0 = self.kind_offsets[i]
+            N.call("lbm_classify", N.C.byref(g), N.ptr(solid), None, 0, N.ptr(self._kind[k0:]), N.ptr(self._nbr[k0:]),
+                   stream)
 
         # ---- descriptors
         dom = (N.Domain * len(self.params))()
@@ -164,8 +160,7 @@ class BatchedSolver:
         self.block, self.blocks = (bx, by), int(blocks)
         self.batch = N.Batch(
             self.grids[0].lattice, self.grids[0].storage, len(self.params), N.ptr(self._domains), len(tiles),
-            N.ptr(self._tiles), int(self._bnode.numel()), N.ptr(self._bdom), N.ptr(self._bnode), bx, by, self.blocks,
-            N.ptr(self._kind), N.ptr(self._wall),
+            N.ptr(self._tiles), bx, by, self.blocks, N.ptr(self._kind), N.ptr(self._nbr), N.ptr(self._wall),
         )
         self._graphs.clear()
 
@@ -185,7 +180,7 @@ class BatchedSolver:
         wall = None
         if self.wall_offsets[i] >= 0:
             wall = self._wall[self.wall_offsets[i] :]
-        return N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(wall), None)
+        return N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(wall), None, N.ptr(self._nbr[self.kind_offsets[i]:]))
 
     # ------------------------------------------------------------------ state
     def initialize(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0, domain: int | None = None) -> None:
@@ -299,21 +294,11 @@ class BatchedSolver:
     def run_separately(self, steps: int) -> None:
         """Reference point: every domain launched on its own every step (no batching, no graphs)."""
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
-        launch = N.Launch(self.block[0], self.block[1], N.LAUNCH_FUSED)
-        specials = []
-        for i, g in enumerate(self.grids):
-            sel = self._bdom == i
-            nodes = self._bnode[sel].contiguous()
-            n = int(nodes.numel())
-            zeros = self.torch.zeros(max(n, 1), dtype=self.torch.int32, device=self.device)
-            minus = self.torch.full((max(n, 1),), -1, dtype=self.torch.int32, device=self.device)
-            sp = N.Special(n, N.ptr(nodes), N.ptr(zeros), N.ptr(zeros), N.ptr(minus), N.ptr(zeros), N.ptr(zeros),
-                           0, 0, None, None, None, None, None, None, None, 0, 0, None, None)
-            specials.append((sp, nodes, zeros, minus))
+        launch = N.Launch(self.block[0], self.block[1], N.LAUNCH_BULK)
         phys = [self._physics(i) for i in range(len(self.grids))]
         for _ in range(steps):
             for i, g in enumerate(self.grids):
-                N.call("lbm_step_pull", N.C.byref(g), N.C.byref(phys[i]), N.C.byref(specials[i][0]), N.C.byref(launch),
+                N.call("lbm_step_pull", N.C.byref(g), N.C.byref(phys[i]), None, N.C.byref(launch),
                        N.ptr(self._kind[self.kind_offsets[i] :]), N.ptr(self._slice(self._f, i)),
                        N.ptr(self._slice(self._g, i)), stream)
             self._f, self._g = self._g, self._f

@@ -18,7 +18,7 @@ static bool grid_valid(const lbm_grid_t* g)
     if (g->storage < LBM_F32 || g->storage > LBM_BF16) return false;
     if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->pitch < g->nx) return false;
     if (g->lattice == LBM_D2Q9 && g->nz != 1) return false;
-    return g->qstride == (int64_t)g->pitch * g->ny * g->nz;
+    return g->qstride >= (int64_t)g->pitch * g->ny * g->nz;
 }
 
 static bool special_valid(const lbm_special_t* sp, bool aa)
@@ -60,6 +60,8 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
     a.f_dst = dst;
     a.wall_u = p->wall_u;
     a.force_field = p->force_field;
+    a.nbr = p->solid_nbr;
+    if (!a.nbr) return LBM_ERR_INVALID;
     if (sp)
         a.sp = *sp;
     else

@@ -160,20 +160,18 @@ struct AdjointKernel {
         finish(A, nd, s, lam);
     }
 
-    // Any fluid node of the adjoint list: bounce-back, wrap, rules, rule-term
-    // and loss gathers.
-    __device__ static __forceinline__ void general(const AdjArgs& A, int64_t s_idx)
+    // Any fluid node that is not interior: bounce-back and wrap; for nodes of
+    // the adjoint list (s_idx >= 0) also rules, rule-term and loss gathers.
+    __device__ static __forceinline__ void general(const AdjArgs& A, int64_t nd, int64_t s_idx)
     {
         const StepArgs& a = A.a;
         const lbm_special_t& sp = a.sp;
-        const int64_t nd = sp.node[s_idx];
         const int64_t row = nd / a.pitch;
         const int x = (int)(nd - row * a.pitch), y = (int)(row % a.ny), z = (int)(row / a.ny);
         const int64_t qs = a.qstride;
-        const uint8_t* kind = a.kind;
-        const bool near = (kind[nd] & KIND_NEAR) != 0;
-        const uint32_t rmask = sp.rule_mask[s_idx];
-        const int rfirst = sp.rule_first[s_idx];
+        const uint32_t bb = a.nbr[nd];
+        const uint32_t rmask = s_idx >= 0 ? sp.rule_mask[s_idx] : 0u;
+        const int rfirst = s_idx >= 0 ? sp.rule_first[s_idx] : 0;
         const int xm = wrap(x - 1, a.nx), xp = wrap(x + 1, a.nx);
         const int ym = wrap(y - 1, a.ny), yp = wrap(y + 1, a.ny);
         const int zm = L::D == 3 ? wrap(z - 1, a.nz) : 0, zp = L::D == 3 ? wrap(z + 1, a.nz) : 0;
@@ -188,7 +186,7 @@ struct AdjointKernel {
             const int sy = L::cy(i) > 0 ? ym : (L::cy(i) < 0 ? yp : y);
             const int sz = L::cz(i) > 0 ? zm : (L::cz(i) < 0 ? zp : z);
             const int64_t src = ((int64_t)sz * a.ny + sy) * a.pitch + sx;
-            if (i != 0 && near && (kind[src] & KIND_SOLID))
+            if (i != 0 && ((bb >> i) & 1u))
                 s[i] = S::load(f + L::opp(i) * qs + nd) + wall_term<L, R>(i, wall, src, qs);
             else
                 s[i] = S::load(f + i * qs + src);
@@ -199,7 +197,7 @@ struct AdjointKernel {
                 const int dy = L::cy(i) > 0 ? yp : (L::cy(i) < 0 ? ym : y);
                 const int dz = L::cz(i) > 0 ? zp : (L::cz(i) < 0 ? zm : z);
                 const int64_t dst = ((int64_t)dz * a.ny + dy) * a.pitch + dx;
-                if (i == 0 || !(kind[dst] & KIND_SOLID))
+                if (i == 0 || !((bb >> L::opp(i)) & 1u))
                     lam[i] = mn[i * qs + dst];
                 else if (!((rmask >> L::opp(i)) & 1u))
                     lam[i] = mn[L::opp(i) * qs + nd];
@@ -223,7 +221,7 @@ struct AdjointKernel {
             }
         }
         // rule-term and loss gathers into lambda
-        {
+        if (s_idx >= 0) {
             const R* gc = static_cast<const R*>(A.adj.gather_coeff);
             const R scale = R(A.loss_scale);
             for (int e = A.adj.gather_start[s_idx]; e < A.adj.gather_start[s_idx + 1]; ++e) {
@@ -267,14 +265,18 @@ __global__ void __launch_bounds__(256) lbm_adjoint_bulk_kernel(const AdjArgs A)
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.nx || y >= a.ny) return;
     const int64_t nd = ((int64_t)blockIdx.z * a.ny + y) * a.pitch + x;
-    if (a.kind[nd] == KIND_FLUID) AdjointKernel<L, ST>::interior(A, nd);
+    const uint8_t k = a.kind[nd];
+    if (k == KIND_FLUID)
+        AdjointKernel<L, ST>::interior(A, nd);
+    else if (!(k & (KIND_SOLID | KIND_SPECIAL)))
+        AdjointKernel<L, ST>::general(A, nd, -1);
 }
 
 template <class L, int ST>
 __global__ void __launch_bounds__(256, 1) lbm_adjoint_boundary_kernel(const AdjArgs A)
 {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (s < A.a.sp.n_special) AdjointKernel<L, ST>::general(A, s);
+    if (s < A.a.sp.n_special) AdjointKernel<L, ST>::general(A, A.a.sp.node[s], s);
 }
 
 template <class L, int ST>
@@ -376,7 +378,7 @@ static bool make_adj(AdjArgs& A, const lbm_grid_t* g, const lbm_physics_t* p, co
                      const lbm_adjoint_t* adj, const uint8_t* kind, const void* f_t, const void* mu_next, void* mu_out,
                      double loss_scale)
 {
-    if (!g || !p || !adj || !kind || g->qstride != (int64_t)g->pitch * g->ny * g->nz || g->pitch < g->nx) return false;
+    if (!g || !p || !adj || !kind || g->qstride < (int64_t)g->pitch * g->ny * g->nz || g->pitch < g->nx) return false;
     if (g->lattice == LBM_D2Q9 && g->nz != 1) return false;
     StepArgs& a = A.a;
     a.nx = g->nx;
@@ -394,6 +396,8 @@ static bool make_adj(AdjArgs& A, const lbm_grid_t* g, const lbm_physics_t* p, co
     a.f_dst = nullptr;
     a.wall_u = p->wall_u;
     a.force_field = p->force_field;
+    a.nbr = p->solid_nbr;
+    if (!a.nbr) return false;
     if (sp)
         a.sp = *sp;
     else

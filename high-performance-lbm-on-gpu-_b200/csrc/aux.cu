@@ -11,13 +11,15 @@ namespace lbm {
 template <class L>
 __device__ __forceinline__ int natural_slot(int i, int layout) { return layout == LBM_LAYOUT_AA_ODD ? L::opp(i) : i; }
 
+// Node coordinates of a pitched index; false for padding (x >= nx, or the
+// tail of a plane padded beyond pitch * ny * nz).
 __device__ __forceinline__ bool decode_node(const lbm_grid_t& g, int64_t nd, int& x, int& y, int& z)
 {
     const int64_t row = nd / g.pitch;
     x = (int)(nd - row * g.pitch);
     y = (int)(row % g.ny);
     z = (int)(row / g.ny);
-    return x < g.nx;
+    return x < g.nx && z < g.nz;
 }
 
 // ---------------------------------------------------------------- init
@@ -102,28 +104,31 @@ int pack(const lbm_grid_t& g, const void* in, int layout, void* f, cudaStream_t 
 
 // ---------------------------------------------------------------- classify
 template <class L>
-__global__ void classify_kernel(const lbm_grid_t g, const uint8_t* __restrict__ solid, uint8_t* __restrict__ kind)
+__global__ void classify_kernel(const lbm_grid_t g, const uint8_t* __restrict__ solid, uint8_t* __restrict__ kind,
+                                uint32_t* __restrict__ nbr)
 {
     const int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (nd >= g.qstride) return;
     int x, y, z;
     if (!decode_node(g, nd, x, y, z)) {
-        kind[nd] = KIND_SOLID;  // padding columns: never updated, never a neighbour
+        kind[nd] = KIND_SOLID;  // padding: never updated, never a neighbour
+        if (nbr) nbr[nd] = 0;
         return;
     }
-    if (solid[nd]) {
-        kind[nd] = KIND_SOLID;
-        return;
-    }
-    bool near = false;
+    uint32_t m = 0;
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
         const int sx = wrap(x - L::cx(i), g.nx), sy = wrap(y - L::cy(i), g.ny);
         const int sz = L::D == 3 ? wrap(z - L::cz(i), g.nz) : 0;
-        near |= solid[((int64_t)sz * g.ny + sy) * g.pitch + sx] != 0;
+        if (solid[((int64_t)sz * g.ny + sy) * g.pitch + sx]) m |= 1u << i;
+    }
+    if (nbr) nbr[nd] = m;
+    if (solid[nd]) {
+        kind[nd] = KIND_SOLID;
+        return;
     }
     const bool edge = x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1 || (L::D == 3 && (z == 0 || z == g.nz - 1));
-    kind[nd] = (near ? KIND_NEAR : KIND_FLUID) | (edge ? KIND_EDGE : KIND_FLUID);
+    kind[nd] = (m ? KIND_NEAR : KIND_FLUID) | (edge ? KIND_EDGE : KIND_FLUID);
 }
 
 __global__ void mark_special_kernel(const int64_t* __restrict__ nodes, int n, uint8_t* kind)
@@ -134,9 +139,9 @@ __global__ void mark_special_kernel(const int64_t* __restrict__ nodes, int n, ui
 
 template <class L, int ST>
 int classify(const lbm_grid_t& g, const uint8_t* solid, const int64_t* special, int n_special, uint8_t* kind,
-             cudaStream_t s)
+             uint32_t* nbr, cudaStream_t s)
 {
-    classify_kernel<L><<<blocks_for(g.qstride, 256), 256, 0, s>>>(g, solid, kind);
+    classify_kernel<L><<<blocks_for(g.qstride, 256), 256, 0, s>>>(g, solid, kind, nbr);
     if (n_special > 0) mark_special_kernel<<<blocks_for(n_special, 256), 256, 0, s>>>(special, n_special, kind);
     return launch_status();
 }
@@ -350,7 +355,7 @@ static bool grid_ok(const lbm_grid_t* g)
     if (g->lattice != LBM_D2Q9 && g->lattice != LBM_D3Q19) return false;
     if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->pitch < g->nx) return false;
     if (g->lattice == LBM_D2Q9 && g->nz != 1) return false;
-    return g->qstride == (int64_t)g->pitch * g->ny * g->nz;
+    return g->qstride >= (int64_t)g->pitch * g->ny * g->nz;
 }
 
 extern "C" int lbm_init_equilibrium(const lbm_grid_t* g, const lbm_physics_t* p, const double* rho, const double* u,
@@ -373,10 +378,10 @@ extern "C" int lbm_pack(const lbm_grid_t* g, const void* in, int32_t layout, voi
 }
 
 extern "C" int lbm_classify(const lbm_grid_t* g, const uint8_t* solid, const int64_t* special, int32_t n_special,
-                            uint8_t* kind, lbm_stream_t stream)
+                            uint8_t* kind, uint32_t* solid_nbr, lbm_stream_t stream)
 {
     if (!grid_ok(g) || !solid || !kind || n_special < 0 || (n_special > 0 && !special)) return LBM_ERR_INVALID;
-    LBM_DISPATCH(g->lattice, g->storage, classify, *g, solid, special, n_special, kind, (cudaStream_t)stream);
+    LBM_DISPATCH(g->lattice, g->storage, classify, *g, solid, special, n_special, kind, solid_nbr, (cudaStream_t)stream);
 }
 
 extern "C" int lbm_macroscopic(const lbm_grid_t* g, const lbm_physics_t* p, const uint8_t* kind, const void* f,

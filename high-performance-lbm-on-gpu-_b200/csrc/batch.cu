@@ -1,12 +1,12 @@
 // Batched domains: many independent lattices of different sizes advanced by
 // one persistent launch per time step.
 //
-// Every block walks the work list round-robin (item = blockIdx.x,
-// blockIdx.x + gridDim.x, ...): bulk tiles of any domain first, then chunks
-// of the cross-domain boundary list. An item rebuilds the step arguments of
-// its domain from the descriptor (a few cached loads) and runs exactly the
-// per-node code of the single-domain step (interior path or general path),
-// so a batched domain evolves bit for bit like the same domain advanced alone.
+// Every block walks the tile list round-robin (item = blockIdx.x,
+// blockIdx.x + gridDim.x, ...). A tile rebuilds the step arguments of its
+// domain from the descriptor (a few cached loads) and runs exactly the
+// per-node code of the single-domain step (interior path, or the general path
+// for nodes next to a wall), so a batched domain evolves bit for bit like the
+// same domain advanced alone.
 // Blocks never wait on each other.
 #include "dispatch.cuh"
 #include "step_kernels.cuh"
@@ -17,14 +17,11 @@ struct BatchArgs {
     const lbm_domain_t* domains;
     const int4* tiles;
     int n_tiles;
-    int n_boundary;
-    const int* bdom;
-    const int64_t* bnode;
     const uint8_t* kind;
+    const uint32_t* nbr;
     const void* wall;
     const void* f_src;
     void* f_dst;
-    int elem;  // storage bytes per element
 };
 
 template <int ST>
@@ -43,6 +40,7 @@ __device__ __forceinline__ StepArgs domain_args(const BatchArgs& b, int d)
     a.fy = D.force[1];
     a.fz = D.force[2];
     a.kind = b.kind + D.kind_offset;
+    a.nbr = b.nbr + D.kind_offset;
     using T = typename Storage<ST>::T;
     using R = typename Storage<ST>::R;
     a.f_src = static_cast<const T*>(b.f_src) + D.offset;
@@ -53,33 +51,20 @@ __device__ __forceinline__ StepArgs domain_args(const BatchArgs& b, int d)
 }
 
 template <class L, int ST>
-__global__ void __launch_bounds__(256) lbm_batch_kernel(const BatchArgs b)
+__global__ void __launch_bounds__(256, 1) lbm_batch_kernel(const BatchArgs b)
 {
-    using K = StepKernel<L, ST, LBM_PULL>;
-    const int threads = blockDim.x * blockDim.y;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int chunks = (b.n_boundary + threads - 1) / threads;
-    const int items = b.n_tiles + chunks;
-    for (int item = blockIdx.x; item < items; item += gridDim.x) {
-        if (item < b.n_tiles) {
-            const int4 t = b.tiles[item];
-            const StepArgs a = domain_args<ST>(b, t.x);
-            const int x = t.y * blockDim.x + threadIdx.x;
-            const int y = t.z * blockDim.y + threadIdx.y;
-            if (x < a.nx && y < a.ny) {
-                const int64_t nd = ((int64_t)t.w * a.ny + y) * a.pitch + x;
-                if (a.kind[nd] == KIND_FLUID) K::interior(a, nd);
-            }
-        } else {
-            const int64_t s = (int64_t)(item - b.n_tiles) * threads + tid;
-            if (s < b.n_boundary) {
-                const StepArgs a = domain_args<ST>(b, b.bdom[s]);
-                const int64_t nd = b.bnode[s];
-                const int64_t row = nd / a.pitch;
-                const int x = (int)(nd - row * a.pitch);
-                K::template node<false>(a, x, (int)(row % a.ny), (int)(row / a.ny), nd,
-                                        (a.kind[nd] & KIND_NEAR) != 0, -1);
-            }
+    for (int item = blockIdx.x; item < b.n_tiles; item += gridDim.x) {
+        const int4 t = b.tiles[item];
+        const StepArgs a = domain_args<ST>(b, t.x);
+        const int x = t.y * blockDim.x + threadIdx.x;
+        const int y = t.z * blockDim.y + threadIdx.y;
+        if (x < a.nx && y < a.ny) {
+            const int64_t nd = ((int64_t)t.w * a.ny + y) * a.pitch + x;
+            const uint8_t k = a.kind[nd];
+            if (k == KIND_FLUID)
+                StepKernel<L, ST, LBM_PULL>::interior(a, nd);
+            else if (!(k & KIND_SOLID))
+                StepKernel<L, ST, LBM_PULL>::template node<false>(a, x, y, t.w, nd, a.nbr[nd], -1);
         }
     }
 }
@@ -91,14 +76,11 @@ int batch_step(const lbm_batch_t& bt, const void* src, void* dst, cudaStream_t s
     b.domains = bt.domains;
     b.tiles = reinterpret_cast<const int4*>(bt.tiles);
     b.n_tiles = bt.n_tiles;
-    b.n_boundary = bt.n_boundary;
-    b.bdom = bt.boundary_domain;
-    b.bnode = bt.boundary_node;
     b.kind = bt.kind;
+    b.nbr = bt.solid_nbr;
     b.wall = bt.wall_u;
     b.f_src = src;
     b.f_dst = dst;
-    b.elem = (int)sizeof(typename Storage<ST>::T);
     lbm_batch_kernel<L, ST><<<bt.blocks, dim3(bt.tile_x, bt.tile_y), 0, s>>>(b);
     return launch_status();
 }
@@ -119,9 +101,9 @@ using namespace lbm;
 
 extern "C" int lbm_batch_step(const lbm_batch_t* bt, const void* f_src, void* f_dst, lbm_stream_t stream)
 {
-    if (!bt || !f_src || !f_dst || f_src == f_dst || !bt->domains || !bt->kind || bt->n_domains <= 0) return LBM_ERR_INVALID;
-    if (bt->n_tiles < 0 || bt->n_boundary < 0 || (bt->n_tiles > 0 && !bt->tiles)) return LBM_ERR_INVALID;
-    if (bt->n_boundary > 0 && (!bt->boundary_domain || !bt->boundary_node)) return LBM_ERR_INVALID;
+    if (!bt || !f_src || !f_dst || f_src == f_dst || !bt->domains || !bt->kind || !bt->solid_nbr || bt->n_domains <= 0)
+        return LBM_ERR_INVALID;
+    if (bt->n_tiles < 0 || (bt->n_tiles > 0 && !bt->tiles)) return LBM_ERR_INVALID;
     if (bt->tile_x <= 0 || bt->tile_y <= 0 || bt->tile_x % 32 || bt->tile_x * bt->tile_y > 256 || bt->blocks <= 0)
         return LBM_ERR_INVALID;
     LBM_DISPATCH(bt->lattice, bt->storage, batch_step, *bt, f_src, f_dst, (cudaStream_t)stream);

@@ -113,6 +113,22 @@ template <> struct Storage<LBM_BF16> {
     __device__ static __forceinline__ R round(R v) { return decode(encode(v)); }
 };
 
+// ---------------------------------------------------------------- arithmetic
+// The collision is written once over a value type V (float or double).
+// Every operation is an explicit round-to-nearest intrinsic, so the compiler
+// never contracts or reorders it differently in different kernels: the bulk,
+// boundary, fused and batched kernels give a node the same bits.
+__device__ __forceinline__ float v_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float v_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float v_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float v_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float v_rcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double v_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double v_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double v_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double v_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double v_rcp(double a) { return __drcp_rn(a); }
+
 // ---------------------------------------------------------------- collision
 // TRT + Guo forcing on one node (reference src/lbm/collision.py:59-88,
 // forcing.py:37-56). With rho = 1 + sum f~, u = (sum c f + F/2)/rho and, for
@@ -128,49 +144,69 @@ template <> struct Storage<LBM_BF16> {
 //   D = 3 w- rho,  G = 3 (1 - w-/2)
 // so each pair costs ~15 operations; the node-level scalars are shared. BGK
 // is w- = w+ (b = 0). The rest population: f*_0 = (1 - w+) f_0 + w_0 A.
-template <class L, class R>
-__device__ __forceinline__ void collide(R (&f)[L::Q], R wp, R wm, R Fx, R Fy, R Fz)
+// u = (j + F/2) / rho uses one reciprocal per node.
+template <class L, class V>
+__device__ __forceinline__ void collide(V (&f)[L::Q], V wp, V wm,
+                                        V Fx, V Fy, V Fz)
 {
-    R drho = f[0], jx = R(0), jy = R(0), jz = R(0);
+    const V zero = V(0);
+    V drho = f[0], jx = zero, jy = zero, jz = zero;
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
-        drho += f[i];
-        if (L::cx(i) > 0) jx += f[i];
-        if (L::cx(i) < 0) jx -= f[i];
-        if (L::cy(i) > 0) jy += f[i];
-        if (L::cy(i) < 0) jy -= f[i];
-        if (L::cz(i) > 0) jz += f[i];
-        if (L::cz(i) < 0) jz -= f[i];
+        drho = v_add(drho, f[i]);
+        if (L::cx(i) > 0) jx = v_add(jx, f[i]);
+        if (L::cx(i) < 0) jx = v_sub(jx, f[i]);
+        if (L::cy(i) > 0) jy = v_add(jy, f[i]);
+        if (L::cy(i) < 0) jy = v_sub(jy, f[i]);
+        if (L::cz(i) > 0) jz = v_add(jz, f[i]);
+        if (L::cz(i) < 0) jz = v_sub(jz, f[i]);
     }
-    const R rho = R(1) + drho;
-    const R inv = R(1) / rho;
-    const R ux = (jx + R(0.5) * Fx) * inv;
-    const R uy = (jy + R(0.5) * Fy) * inv;
-    const R uz = L::D == 3 ? (jz + R(0.5) * Fz) * inv : R(0);
-    const R usq = ux * ux + uy * uy + uz * uz;
-    const R uF = ux * Fx + uy * Fy + (L::D == 3 ? uz * Fz : R(0));
-    const R ap = R(1) - R(0.5) * wp;
-    const R am = R(1) - R(0.5) * wm;
-    const R A = wp * (drho - R(1.5) * rho * usq) - R(3) * ap * uF;
-    const R B = R(4.5) * wp * rho;
-    const R C = R(9) * ap;
-    const R Dm = R(3) * wm * rho;
-    const R G = R(3) * am;
-    const R ca = R(1) - R(0.5) * (wp + wm);
-    const R cb = R(0.5) * (wm - wp);
-    f[0] = (R(1) - wp) * f[0] + R(L::w(0)) * A;
+    const V half = V(0.5);
+    const V rho = v_add(V(1), drho);
+    const V inv = v_rcp(rho);
+    const V ux = v_mul(v_fma(half, Fx, jx), inv);
+    const V uy = v_mul(v_fma(half, Fy, jy), inv);
+    const V uz = L::D == 3 ? v_mul(v_fma(half, Fz, jz), inv) : zero;
+    V usq = v_mul(ux, ux);
+    usq = v_fma(uy, uy, usq);
+    if (L::D == 3) usq = v_fma(uz, uz, usq);
+    V uF = v_mul(ux, Fx);
+    uF = v_fma(uy, Fy, uF);
+    if (L::D == 3) uF = v_fma(uz, Fz, uF);
+    // Node-independent constants, also with explicit rounding: a contracted
+    // 1 - w/2 in one kernel and an uncontracted one in another would differ.
+    const V ap = v_sub(V(1), v_mul(V(0.5), wp)), am = v_sub(V(1), v_mul(V(0.5), wm));
+    // A = w+ (drho - 1.5 rho usq) - 3 ap uF
+    const V A = v_fma(v_mul(V(-3), ap), uF, v_mul(wp, v_fma(v_mul(V(-1.5), rho), usq, drho)));
+    const V B = v_mul(v_mul(V(4.5), wp), rho);
+    const V C = v_mul(V(9), ap);
+    const V Dm = v_mul(v_mul(V(3), wm), rho);
+    const V G = v_mul(V(3), am);
+    const V ca = v_sub(V(1), v_mul(V(0.5), v_add(wp, wm)));
+    const V cb = v_mul(V(0.5), v_sub(wm, wp));
+    f[0] = v_fma(v_sub(V(1), wp), f[0], v_mul(V(L::w(0)), A));
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
         const int o = L::opp(i);
         if (o < i) continue;
-        const R wi = R(L::w(i));
-        const R cu = R(L::cx(i)) * ux + R(L::cy(i)) * uy + R(L::cz(i)) * uz;
-        const R cF = R(L::cx(i)) * Fx + R(L::cy(i)) * Fy + R(L::cz(i)) * Fz;
-        const R E = wi * (A + cu * (B * cu + C * cF));
-        const R O = wi * (Dm * cu + G * cF);
-        const R fi = f[i], fo = f[o];
-        f[i] = ca * fi + (cb * fo + (E + O));
-        f[o] = ca * fo + (cb * fi + (E - O));
+        const V wi = V(L::w(i));
+        // cu, cF: sums of +-components (exact sign flips, no multiplies)
+        V cu = zero, cF = zero;
+        bool first = true;
+        if (L::cx(i) != 0) { cu = L::cx(i) > 0 ? ux : v_sub(zero, ux); cF = L::cx(i) > 0 ? Fx : v_sub(zero, Fx); first = false; }
+        if (L::cy(i) != 0) {
+            if (first) { cu = L::cy(i) > 0 ? uy : v_sub(zero, uy); cF = L::cy(i) > 0 ? Fy : v_sub(zero, Fy); first = false; }
+            else { cu = L::cy(i) > 0 ? v_add(cu, uy) : v_sub(cu, uy); cF = L::cy(i) > 0 ? v_add(cF, Fy) : v_sub(cF, Fy); }
+        }
+        if (L::cz(i) != 0) {
+            if (first) { cu = L::cz(i) > 0 ? uz : v_sub(zero, uz); cF = L::cz(i) > 0 ? Fz : v_sub(zero, Fz); }
+            else { cu = L::cz(i) > 0 ? v_add(cu, uz) : v_sub(cu, uz); cF = L::cz(i) > 0 ? v_add(cF, Fz) : v_sub(cF, Fz); }
+        }
+        const V E = v_mul(wi, v_fma(cu, v_fma(B, cu, v_mul(C, cF)), A));
+        const V O = v_mul(wi, v_fma(Dm, cu, v_mul(G, cF)));
+        const V fi = f[i], fo = f[o];
+        f[i] = v_fma(ca, fi, v_fma(cb, fo, v_add(E, O)));
+        f[o] = v_fma(ca, fo, v_fma(cb, fi, v_sub(E, O)));
     }
 }
 
@@ -200,8 +236,8 @@ struct StepArgs {
     void* f_dst;
     const void* wall_u;
     const void* force_field;
+    const uint32_t* nbr;  // solid-neighbour mask per node
     lbm_special_t sp;
-    int32_t* status;
 };
 
 }  // namespace lbm

@@ -4,12 +4,13 @@
 // One launch updates every fluid node once:
 //   * bulk blocks: a (tile_x x tile_y) tile of one z plane, one node per
 //     thread. Interior nodes (kind 0) stream with fixed, warp-uniform
-//     offsets and no branch; every other node returns.
-//   * boundary warps: one thread per entry of the compact list of all other
-//     fluid nodes -- next to a wall (bounce-back, Ladd term), on a periodic
-//     face (wrap), carrying link rules, an immersed-boundary force or AA
-//     rule-term exports. Rules are evaluated in registers while the node
-//     is updated, so they need no pre-pass launch and no scatter.
+//     offsets and no branch; nodes next to a wall or on a periodic face take
+//     the general path, driven by the precomputed solid-neighbour mask (no
+//     neighbour kind is loaded, so all loads stay independent).
+//   * boundary warps: one thread per SPECIAL node of the compact list --
+//     carrying link rules, an immersed-boundary force or AA rule-term
+//     exports. Rules are evaluated in registers while the node is updated,
+//     so they need no pre-pass launch and no scatter.
 //   The boundary warps run in the same launch (FUSED) or as a second kernel
 //   that may overlap the bulk (BULK + BOUNDARY); see lbm_launch_t.
 //
@@ -25,6 +26,8 @@
 //   collision, and the next launch evaluates its rules from that copy
 //   (export_in). The two export buffers alternate between launches.
 #pragma once
+
+#include <type_traits>
 
 #include "lbm_common.cuh"
 
@@ -99,10 +102,12 @@ struct StepKernel {
         }
     }
 
+    // General path: bb = solid-neighbour mask (bit i: x - c_i is solid, so
+    // bit opp(i): x + c_i is solid). No kind byte of a neighbour is loaded,
+    // so all Q loads are independent.
     template <bool SPECIAL>
-    __device__ static __forceinline__ void node(const StepArgs& a, int x, int y, int z, int64_t nd, bool near, int64_t s)
+    __device__ static __forceinline__ void node(const StepArgs& a, int x, int y, int z, int64_t nd, uint32_t bb, int64_t s)
     {
-        const uint8_t* __restrict__ kind = a.kind;
         const int64_t qs = a.qstride;
         const R* __restrict__ wall = static_cast<const R*>(a.wall_u);
         uint32_t rmask = 0;
@@ -129,7 +134,7 @@ struct StepKernel {
             const int sz = L::cz(i) > 0 ? zm : (L::cz(i) < 0 ? zp : z);
             const int64_t src = ((int64_t)sz * a.ny + sy) * a.pitch + sx;
             const T* fs = static_cast<const T*>(a.f_src);
-            if (i != 0 && near && (kind[src] & KIND_SOLID)) {
+            if (i != 0 && ((bb >> i) & 1u)) {
                 // halfway bounce-back: the population that left x towards the wall
                 const int slot = VAR == LBM_PULL ? L::opp(i) : i;
                 f[i] = S::load(fs + slot * qs + nd) + wall_term<L, R>(i, wall, src, qs);
@@ -191,7 +196,7 @@ struct StepKernel {
                 const int dy = L::cy(i) > 0 ? yp : (L::cy(i) < 0 ? ym : y);
                 const int dz = L::cz(i) > 0 ? zp : (L::cz(i) < 0 ? zm : z);
                 const int64_t dst = ((int64_t)dz * a.ny + dy) * a.pitch + dx;
-                if (i != 0 && near && (kind[dst] & KIND_SOLID)) {
+                if (i != 0 && ((bb >> L::opp(i)) & 1u)) {
                     S::store(fd + L::opp(i) * qs + nd, f[i] + wall_term<L, R>(L::opp(i), wall, dst, qs));
                 } else {
                     S::store(fd + i * qs + dst, f[i]);
@@ -229,7 +234,11 @@ __device__ __forceinline__ void bulk_tile(const StepArgs& a, int z)
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.nx || y >= a.ny) return;
     const int64_t nd = ((int64_t)z * a.ny + y) * a.pitch + x;
-    if (a.kind[nd] == KIND_FLUID) StepKernel<L, ST, VAR>::interior(a, nd);
+    const uint8_t k = a.kind[nd];
+    if (k == KIND_FLUID)
+        StepKernel<L, ST, VAR>::interior(a, nd);
+    else if (!(k & (KIND_SOLID | KIND_SPECIAL)))
+        StepKernel<L, ST, VAR>::template node<false>(a, x, y, z, nd, a.nbr[nd], -1);
 }
 
 template <class L, int ST, int VAR>
@@ -241,11 +250,9 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
     const int x = (int)(nd - row * a.pitch);
     const int y = (int)(row % a.ny);
     const int z = (int)(row / a.ny);
-    StepKernel<L, ST, VAR>::template node<true>(a, x, y, z, nd, (a.kind[nd] & KIND_NEAR) != 0, s);
+    StepKernel<L, ST, VAR>::template node<true>(a, x, y, z, nd, a.nbr[nd], s);
 }
 
-// FUSED: grid (ceil(nx/bx), ceil(ny/by), nz + extra); planes z >= nz are
-// boundary warps. BULK: the same grid without the extra planes.
 // Bulk-only launches: ptxas's default register target (no spills, high
 // occupancy) -- this kernel carries almost all of the traffic.
 template <class L, int ST, int VAR>

@@ -214,7 +214,7 @@ class CudaSolver(Solver):
         self.grid = N.Grid(N.LATTICE_CODE[lattice.name], N.STORAGE_CODE[self.storage], nx, ny, nz, self.pitch, self.qstride)
         self.launch_mode = launch
         self.keep_zero_terms = bool(keep_zero_terms)
-        self._launches = {m: N.Launch(bx, by, m) for m in (N.LAUNCH_FUSED, N.LAUNCH_BULK, N.LAUNCH_BOUNDARY)}
+        self._launches = {m: N.Launch(bx, by, m) for m in N.LAUNCH_MODES}
         self.block = (bx, by)
 
         # ---- physics
@@ -225,7 +225,7 @@ class CudaSolver(Solver):
         self._force_field = None
         if force_field is not None:
             self._force_field = self._upload_field(np.asarray(force_field, dtype=np.float64).reshape(d, *shape))
-        self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field))
+        self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field), None)
 
         # ---- immersed boundary and link rules -> special nodes
         self._ibm = None
@@ -282,9 +282,10 @@ class CudaSolver(Solver):
     def _build_special(self, params) -> _SpecialTables:
         """Classify the nodes on the device and build the boundary-warp list.
 
-        The list holds every fluid node that is not interior: next to a wall,
-        on a periodic face, carrying link rules, an immersed-boundary force or
-        (AA) rule-term exports. Rules are sorted by (node, direction).
+        The list holds the SPECIAL nodes: those carrying link rules, an
+        immersed-boundary force or (AA) rule-term exports. Nodes that are only
+        next to a wall or on a periodic face stay with the bulk kernel, which
+        reads their solid-neighbour mask. Rules are sorted by (node, direction).
         """
         torch = self.torch
         lat = self.lattice
@@ -335,21 +336,20 @@ class CudaSolver(Solver):
             t["export_a"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
             t["export_b"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
 
-        # ---- node kinds on the device; marked nodes get the SPECIAL bit
-        marked = np.unique(np.concatenate([rule_nodes, ibm_nodes, export_nodes]))
-        marked_t = torch.from_numpy(marked).to(self.device) if marked.size else None
+        # ---- node kinds and solid-neighbour masks on the device; marked nodes get the SPECIAL bit
+        nodes = np.unique(np.concatenate([rule_nodes, ibm_nodes, export_nodes])).astype(np.int64)
+        marked_t = torch.from_numpy(nodes).to(self.device) if nodes.size else None
         solid = self._upload_scalar(self._solid_host.astype(np.uint8), torch.uint8)
         self._kind = torch.empty(self.qstride, dtype=torch.uint8, device=self.device)
-        self._native("lbm_classify", N.C.byref(self.grid), N.ptr(solid), N.ptr(marked_t), int(marked.size),
-                     N.ptr(self._kind), self._stream())
-        k = self._kind
-        listed = torch.nonzero((k != 0) & ((k & N.KIND_SOLID) == 0)).flatten()
-        nodes = listed.cpu().numpy().astype(np.int64)  # ascending pitched indices
+        self._nbr = torch.empty(self.qstride, dtype=torch.int32, device=self.device)
+        self._native("lbm_classify", N.C.byref(self.grid), N.ptr(solid), N.ptr(marked_t), int(nodes.size),
+                     N.ptr(self._kind), N.ptr(self._nbr), self._stream())
+        self.physics.solid_nbr = N.ptr(self._nbr)
         ns = nodes.size
         if ns == 0:
             return _SpecialTables({}, 0, 0, 0, 0, 0)
         if ns >= 2**31:
-            raise ValueError("too many boundary nodes")
+            raise ValueError("too many special nodes")
         rule_mask = np.zeros(ns, dtype=np.uint32)
         rule_first = np.zeros(ns, dtype=np.int32)
         if n_rules:
@@ -365,7 +365,7 @@ class CudaSolver(Solver):
             pos = np.searchsorted(nodes, export_nodes)
             np.bitwise_or.at(export_mask, pos, (np.uint32(1) << export_dirs.astype(np.uint32)))
             export_first = np.searchsorted(export_nodes, nodes, side="left").astype(np.int32)
-        t["node"] = listed.contiguous()
+        t["node"] = marked_t
         t["rule_mask"] = torch.from_numpy(rule_mask.view(np.int32)).to(self.device)
         t["rule_first"] = torch.from_numpy(rule_first).to(self.device)
         t["force_slot"] = torch.from_numpy(force_slot).to(self.device)
@@ -491,7 +491,7 @@ class CudaSolver(Solver):
         """One time step: a fused launch, or bulk + boundary kernels forked onto two streams."""
         g, ph = N.C.byref(self.grid), N.C.byref(self.physics)
         if self.launch_mode == "fused" or self._special.n_special == 0:
-            mode = N.LAUNCH_FUSED if self._special.n_special else N.LAUNCH_BULK
+            mode = N.LAUNCH_FUSED if (self._special.n_special and self.launch_mode == "fused") else N.LAUNCH_BULK
             self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[mode]), N.ptr(self._kind), *tail,
                          self._stream())
             return
@@ -666,7 +666,8 @@ class CudaSolver(Solver):
         """Registers, spill bytes and shared memory of the step kernels (``cuda_solver.py:311-326``)."""
         lib = N.load()
         variants = {"aa_odd": N.LBM_AA_ODD, "aa_even": N.LBM_AA_EVEN} if self.variant == "aa" else {"pull": N.LBM_PULL}
-        modes = {"fused": N.LAUNCH_FUSED} if self.launch_mode == "fused" else {"bulk": N.LAUNCH_BULK, "boundary": N.LAUNCH_BOUNDARY}
+        modes = {"fused": N.LAUNCH_FUSED} if self.launch_mode == "fused" else {"bulk": N.LAUNCH_BULK,
+                                                                               "boundary": N.LAUNCH_BOUNDARY}
         out = {}
         for vname, code in variants.items():
             for mname, mode in modes.items():

@@ -49,7 +49,7 @@ typedef struct lbm_grid {
     int32_t storage;   /* LBM_F32, LBM_F64, LBM_F16, LBM_BF16 */
     int32_t nx, ny, nz;
     int32_t pitch;     /* row pitch in nodes, >= nx */
-    int64_t qstride;   /* pitch * ny * nz */
+    int64_t qstride;   /* elements between direction planes, >= pitch * ny * nz */
 } lbm_grid_t;
 
 /* Collision constants and wall data. "real" arrays use the compute type:
@@ -60,6 +60,8 @@ typedef struct lbm_physics {
     double force[3];       /* uniform body-force density */
     const void* wall_u;    /* real[d][qstride] wall velocity at solid nodes, or NULL (all walls at rest) */
     const void* force_field; /* real[d][qstride] per-node body force added to force[], or NULL */
+    const uint32_t* solid_nbr; /* per node: bit i set where x - c_i is solid (lbm_classify); read only
+                                  at fluid nodes that are not interior */
 } lbm_physics_t;
 
 /* Nodes updated by the boundary warps, and the link rules they apply.
@@ -89,11 +91,13 @@ typedef struct lbm_special {
     void* export_out;             /* AA: real[n_export] read by the next launch */
 } lbm_special_t;
 
-/* How a step is launched. The bulk grid covers the interior fluid nodes
- * (kind 0) with blocks of tile_x * tile_y threads, one node each, over
- * (ceil(nx/tile_x), ceil(ny/tile_y), nz). Every other fluid node (near a
- * wall, on a periodic face, with rules, an immersed-boundary force or
- * exports) must be in the special list and is updated by the boundary warps:
+/* How a step is launched. The bulk grid covers every fluid node that is not
+ * SPECIAL with blocks of tile_x * tile_y threads, one node each, over
+ * (ceil(nx/tile_x), ceil(ny/tile_y), nz): interior nodes (kind 0) stream with
+ * fixed offsets, nodes next to a wall or on a periodic face take the general
+ * path driven by phys->solid_nbr. SPECIAL nodes (link rules, an
+ * immersed-boundary force, AA exports) must be in the special list and are
+ * updated by the boundary warps:
  *   LBM_LAUNCH_FUSED    one launch, boundary warps in extra z-planes of blocks;
  *   LBM_LAUNCH_BULK     the bulk grid only;
  *   LBM_LAUNCH_BOUNDARY the boundary warps only (1D grid over the list).
@@ -135,9 +139,10 @@ int lbm_export_prime(const lbm_grid_t* grid, const lbm_special_t* sp, const void
 /* ---- node kinds -------------------------------------------------------- */
 
 /* kind[node] = SOLID | SPECIAL | NEAR | EDGE from a solid mask (uint8, 0/1, pitched
- * like the lattice) and a list of special nodes. Periodic neighbours. */
+ * like the lattice) and a list of special nodes; solid_nbr[node] = bit i set
+ * where node - c_i is solid (periodic neighbours), or NULL to skip it. */
 int lbm_classify(const lbm_grid_t* grid, const uint8_t* solid, const int64_t* special_nodes,
-                 int32_t n_special, uint8_t* kind, lbm_stream_t stream);
+                 int32_t n_special, uint8_t* kind, uint32_t* solid_nbr, lbm_stream_t stream);
 
 /* ---- state conversion ------------------------------------------------- */
 
@@ -275,23 +280,21 @@ typedef struct lbm_domain {
     double force[3];
 } lbm_domain_t;
 
-/* Work list of a batch step: n_tiles bulk tiles, each int32 x4 = (domain,
- * tile index along x, tile index along y, z), then the boundary list (every
- * non-interior fluid node of every domain) in chunks of tile_x * tile_y.
- * A persistent grid of `blocks` blocks walks the items round-robin; no block
- * waits for another. */
+/* Work list of a batch step: n_tiles tiles, each int32 x4 = (domain, tile
+ * index along x, tile index along y, z). A persistent grid of `blocks` blocks
+ * walks the tiles round-robin; no block waits for another. Every fluid node
+ * of a tile is updated (interior path, or the general path for nodes next to
+ * a wall or on a periodic face). */
 typedef struct lbm_batch {
     int32_t lattice, storage;
     int32_t n_domains;
     const lbm_domain_t* domains;   /* device array */
     int32_t n_tiles;
     const int32_t* tiles;          /* device, 4 int32 per tile */
-    int32_t n_boundary;
-    const int32_t* boundary_domain;  /* device */
-    const int64_t* boundary_node;    /* device, pitched node index inside the domain */
     int32_t tile_x, tile_y;        /* tile_x multiple of 32, tile_x * tile_y <= 256 */
     int32_t blocks;                /* persistent grid size (> 0) */
-    const uint8_t* kind;           /* kind pool */
+    const uint8_t* kind;           /* kind pool (domain i at kind_offset) */
+    const uint32_t* solid_nbr;     /* solid-neighbour pool, same offsets as kind */
     const void* wall_u;            /* wall pool (compute type) or NULL */
 } lbm_batch_t;
 

@@ -56,7 +56,8 @@ def test_device_lattice_tables_match_python(tmp_path):
     )
     exe = tmp_path / "tables"
     csrc = ROOT / "high-performance-lbm-on-gpu-_b200" / "csrc"
-    subprocess.run(["nvcc", "-std=c++17", f"-I{csrc}", str(src), "-o", str(exe)], check=True, capture_output=True)
+    subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", f"-I{csrc}", str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
     rows = [line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()]
     for vs, block in ((lbm.D2Q9, rows[:9]), (lbm.D3Q19, rows[9:])):
         c = np.array([[int(r[0]), int(r[1]), int(r[2])] for r in block])
