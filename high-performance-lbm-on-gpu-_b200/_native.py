@@ -13,7 +13,8 @@ HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
 ABI_VERSION = 1
 
-LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH = 0, -1, -2, -3
+LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
+AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
 LBM_D2Q9, LBM_D3Q19 = 0, 1
 LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
 LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
@@ -109,6 +110,7 @@ _SIGNATURES = {
     "lbm_health": [P(Grid), vp, vp, vp, vp],
     "lbm_affine_gather": [i32, vp, vp, vp, vp, i64, i32, vp, vp],
     "lbm_affine_reduce": [i32, vp, vp, vp, vp, vp, i64, i32, i32, vp, vp, vp, vp],
+    "lbm_affine_reduce_static": [i32, vp, vp, vp, vp, vp, i64, i32, i32, vp, vp],
     "lbm_ibm_moments": [P(Grid), P(Physics), P(Ibm), vp, i32, vp],
     "lbm_ibm_iteration": [P(Grid), P(Ibm), i32, vp, vp, vp],
     "lbm_ibm_body_force": [P(Grid), P(Ibm), i32, vp, vp],
@@ -154,6 +156,8 @@ def check(status: int, what: str) -> None:
         raise NativeError(f"{what}: CUDA launch failed ({lib.lbm_last_cuda_error().decode()})")
     if status == LBM_ERR_UNSUPPORTED:
         raise NativeError(f"{what}: unsupported configuration")
+    if status == LBM_ERR_TOO_LARGE:
+        raise NativeError(f"{what}: size beyond the library's fixed scratch limit")
     raise NativeError(f"{what}: invalid argument (status {status})")
 
 

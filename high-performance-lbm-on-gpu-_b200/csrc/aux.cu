@@ -2,6 +2,7 @@
 // node classification, macroscopic readout, divergence watchdog, affine
 // gathers/reductions (force probes) and the AA rule-term export priming.
 #include <climits>
+#include <mutex>
 
 #include "dispatch.cuh"
 
@@ -459,6 +460,58 @@ extern "C" int lbm_affine_reduce(int32_t storage, const void* f, const int64_t* 
     case LBM_BF16: return affine_reduce_t<LBM_BF16>(f, slots, coeff, constant, weight, n_rows, n_terms, d, partial, counter, out, s);
     default: return LBM_ERR_INVALID;
     }
+}
+
+// ---------------------------------------------------------------- affine reduce, no allocation
+// lbm_affine_reduce_static runs affine_reduce_kernel with its scratch in this
+// fixed array instead of caller buffers: a 256-byte head whose first word is
+// the block counter, then partial[block][a] for up to
+// LBM_AFFINE_REDUCE_STATIC_MAX_ROWS rows (3 doubles per 256-row block).
+// Size: 256 B + 4096 * 3 * 8 B = 96.25 KiB per device.
+constexpr int64_t kStaticReduceBlocks = (LBM_AFFINE_REDUCE_STATIC_MAX_ROWS + 255) / 256;
+constexpr int64_t kStaticReduceHead = 32;  // doubles: 256 bytes
+static __device__ __align__(256) double g_reduce_scratch[kStaticReduceHead + kStaticReduceBlocks * 3];
+
+// Device address of g_reduce_scratch, looked up once per device (with that
+// device current) and cached; the lookup may load this library's device code.
+constexpr int kMaxDevices = 64;
+static std::mutex g_scratch_mutex;
+static double* g_scratch_ptr[kMaxDevices];
+
+static int static_reduce_scratch(double** out)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LBM_ERR_LAUNCH;
+    if (dev < 0 || dev >= kMaxDevices) return LBM_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (g_scratch_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_reduce_scratch) != cudaSuccess || p == nullptr) return LBM_ERR_LAUNCH;
+        g_scratch_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return LBM_OK;
+}
+
+extern "C" int lbm_affine_reduce_static(int32_t storage, const void* f, const int64_t* slots, const double* coeff,
+                                        const double* constant, const double* weight, int64_t n_rows,
+                                        int32_t n_terms, int32_t d, double* out, lbm_stream_t stream)
+{
+    if (!f || n_rows <= 0 || n_terms < 0 || d < 1 || d > 3 || !slots || !coeff || !constant || !weight || !out)
+        return LBM_ERR_INVALID;
+    if (storage < LBM_F32 || storage > LBM_BF16) return LBM_ERR_INVALID;
+    if (n_rows > LBM_AFFINE_REDUCE_STATIC_MAX_ROWS) return LBM_ERR_TOO_LARGE;
+    double* scratch = nullptr;
+    const int status = static_reduce_scratch(&scratch);
+    if (status != LBM_OK) return status;
+    uint32_t* counter = reinterpret_cast<uint32_t*>(scratch);
+    double* partial = scratch + kStaticReduceHead;
+    cudaStream_t s = (cudaStream_t)stream;
+    // The kernel's last block re-arms the counter; clearing it here as well
+    // keeps a call correct whatever state an earlier failed launch left.
+    if (cudaMemsetAsync(counter, 0, sizeof(uint32_t), s) != cudaSuccess) return LBM_ERR_LAUNCH;
+    return lbm_affine_reduce(storage, f, slots, coeff, constant, weight, n_rows, n_terms, d, partial, counter, out,
+                             stream);
 }
 
 extern "C" int lbm_export_prime(const lbm_grid_t* g, const lbm_special_t* sp, const void* f, int32_t layout,

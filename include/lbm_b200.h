@@ -29,7 +29,8 @@ enum {
     LBM_OK = 0,
     LBM_ERR_INVALID = -1,      /* bad argument (null pointer, size, enum)   */
     LBM_ERR_UNSUPPORTED = -2,  /* combination not built into this library   */
-    LBM_ERR_LAUNCH = -3        /* kernel launch failed; see lbm_last_cuda_error */
+    LBM_ERR_LAUNCH = -3,       /* kernel launch failed; see lbm_last_cuda_error */
+    LBM_ERR_TOO_LARGE = -4     /* size beyond a fixed in-library scratch limit */
 };
 
 /* ---- enums ------------------------------------------------------------ */
@@ -195,6 +196,29 @@ int lbm_affine_gather(int32_t storage, const void* f, const int64_t* slots, cons
 int lbm_affine_reduce(int32_t storage, const void* f, const int64_t* slots, const double* coeff,
                       const double* constant, const double* weight, int64_t n_rows, int32_t n_terms,
                       int32_t d, double* partial, uint32_t* counter, double* out, lbm_stream_t stream);
+
+/* No-allocation variant of lbm_affine_reduce (no counterpart in the
+ * reference, which reduces probe forces on the host). Same arguments, result
+ * and summation order, minus partial and counter: the scratch is a fixed
+ * array inside this library (96.25 KiB per device), so the call allocates
+ * nothing and needs no buffers beyond its inputs and out[d].
+ * For callers that cannot allocate device memory at the point of the call:
+ * a C or Fortran host that owns only the lattice buffers and has no device
+ * allocator, or a force readout between the launches of a running step loop,
+ * where a cudaMalloc would synchronize the whole device.
+ * Limit: n_rows <= LBM_AFFINE_REDUCE_STATIC_MAX_ROWS; a larger n_rows returns
+ * LBM_ERR_TOO_LARGE and launches nothing (use lbm_affine_reduce instead).
+ * Set-up: the first call on each device, made with that device current,
+ * looks up the array's address and caches it (this may load the library's
+ * device code); make that first call before any stream capture.
+ * Calls share one array per device: calls that may overlap in time on the
+ * same device (different streams, or host threads without ordering) race
+ * and give wrong sums; issue them on one stream. Each call clears the block
+ * counter on its stream before the reduction. */
+#define LBM_AFFINE_REDUCE_STATIC_MAX_ROWS 1048576
+int lbm_affine_reduce_static(int32_t storage, const void* f, const int64_t* slots, const double* coeff,
+                             const double* constant, const double* weight, int64_t n_rows, int32_t n_terms,
+                             int32_t d, double* out, lbm_stream_t stream);
 
 /* ---- immersed boundary (direct forcing, multi-direct) ------------------- */
 /* Replaces ImmersedForcing.force_field (src/lbm/ibm.py:189-214). */
