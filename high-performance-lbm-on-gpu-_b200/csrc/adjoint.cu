@@ -187,7 +187,7 @@ struct AdjointKernel {
             const int sz = L::cz(i) > 0 ? zm : (L::cz(i) < 0 ? zp : z);
             const int64_t src = ((int64_t)sz * a.ny + sy) * a.pitch + sx;
             if (i != 0 && ((bb >> i) & 1u))
-                s[i] = S::load(f + L::opp(i) * qs + nd) + wall_term<L, R>(i, wall, src, qs);
+                s[i] = v_add(S::load(f + L::opp(i) * qs + nd), wall_term<L, R>(i, wall, src, qs));
             else
                 s[i] = S::load(f + i * qs + src);
             // backward: lambda_i from x + c_i

@@ -4,9 +4,8 @@
 // Every block walks the tile list round-robin (item = blockIdx.x,
 // blockIdx.x + gridDim.x, ...). A tile rebuilds the step arguments of its
 // domain from the descriptor (a few cached loads) and runs exactly the
-// per-node code of the single-domain step (interior path, or the general path
-// for nodes next to a wall), so a batched domain evolves bit for bit like the
-// same domain advanced alone.
+// per-node code of the single-domain step (bulk_node), so a batched domain
+// evolves bit for bit like the same domain advanced alone.
 // Blocks never wait on each other.
 #include "dispatch.cuh"
 #include "step_kernels.cuh"
@@ -58,14 +57,7 @@ __global__ void __launch_bounds__(256, 1) lbm_batch_kernel(const BatchArgs b)
         const StepArgs a = domain_args<ST>(b, t.x);
         const int x = t.y * blockDim.x + threadIdx.x;
         const int y = t.z * blockDim.y + threadIdx.y;
-        if (x < a.nx && y < a.ny) {
-            const int64_t nd = ((int64_t)t.w * a.ny + y) * a.pitch + x;
-            const uint8_t k = a.kind[nd];
-            if (k == KIND_FLUID)
-                StepKernel<L, ST, LBM_PULL>::interior(a, nd);
-            else if (!(k & KIND_SOLID))
-                StepKernel<L, ST, LBM_PULL>::template node<false>(a, x, y, t.w, nd, a.nbr[nd], -1);
-        }
+        bulk_node<L, ST, LBM_PULL>(a, x, y, t.w, ((int64_t)t.w * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny);
     }
 }
 

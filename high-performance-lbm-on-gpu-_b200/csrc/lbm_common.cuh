@@ -210,16 +210,18 @@ __device__ __forceinline__ void collide(V (&f)[L::Q], V wp, V wm,
     }
 }
 
-// Moving-wall (Ladd) term 6 w_i (c_i . u_w) with u_w read at solid node s.
+// Moving-wall (Ladd) term 6 w_i (c_i . u_w) with u_w read at solid node s,
+// in explicitly rounded operations (added with v_add by every caller), so
+// every kernel that applies it gives the same bits.
 template <class L, class R>
 __device__ __forceinline__ R wall_term(int i, const R* __restrict__ wall_u, int64_t s, int64_t qstride)
 {
     if (wall_u == nullptr) return R(0);
     R cu = R(0);
-    if (L::cx(i) != 0) cu += R(L::cx(i)) * wall_u[s];
-    if (L::cy(i) != 0) cu += R(L::cy(i)) * wall_u[qstride + s];
-    if (L::D == 3 && L::cz(i) != 0) cu += R(L::cz(i)) * wall_u[2 * qstride + s];
-    return R(6) * R(L::w(i)) * cu;
+    if (L::cx(i) != 0) cu = v_add(cu, v_mul(R(L::cx(i)), wall_u[s]));
+    if (L::cy(i) != 0) cu = v_add(cu, v_mul(R(L::cy(i)), wall_u[qstride + s]));
+    if (L::D == 3 && L::cz(i) != 0) cu = v_add(cu, v_mul(R(L::cz(i)), wall_u[2 * qstride + s]));
+    return v_mul(R(6.0 * L::w(i)), cu);
 }
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }

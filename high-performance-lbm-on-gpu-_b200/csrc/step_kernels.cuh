@@ -3,10 +3,11 @@
 //
 // One launch updates every fluid node once:
 //   * bulk blocks: a (tile_x x tile_y) tile of one z plane, one node per
-//     thread. Interior nodes (kind 0) stream with fixed, warp-uniform
-//     offsets and no branch; nodes next to a wall or on a periodic face take
-//     the general path, driven by the precomputed solid-neighbour mask (no
-//     neighbour kind is loaded, so all loads stay independent).
+//     thread. Warps of interior nodes (kind 0) stream with fixed,
+//     warp-uniform offsets and no branch; a warp with a node next to a wall
+//     or on a periodic face takes the general path on all its lanes, driven
+//     by the precomputed solid-neighbour mask (no neighbour kind is loaded,
+//     so all loads stay independent).
 //   * boundary warps: one thread per SPECIAL node of the compact list --
 //     carrying link rules, an immersed-boundary force or AA rule-term
 //     exports. Rules are evaluated in registers while the node is updated,
@@ -137,7 +138,7 @@ struct StepKernel {
             if (i != 0 && ((bb >> i) & 1u)) {
                 // halfway bounce-back: the population that left x towards the wall
                 const int slot = VAR == LBM_PULL ? L::opp(i) : i;
-                f[i] = S::load(fs + slot * qs + nd) + wall_term<L, R>(i, wall, src, qs);
+                f[i] = v_add(S::load(fs + slot * qs + nd), wall_term<L, R>(i, wall, src, qs));
             } else if (VAR == LBM_PULL) {
                 f[i] = S::load_nc(fs + i * qs + src);
             } else {
@@ -197,7 +198,7 @@ struct StepKernel {
                 const int dz = L::cz(i) > 0 ? zp : (L::cz(i) < 0 ? zm : z);
                 const int64_t dst = ((int64_t)dz * a.ny + dy) * a.pitch + dx;
                 if (i != 0 && ((bb >> L::opp(i)) & 1u)) {
-                    S::store(fd + L::opp(i) * qs + nd, f[i] + wall_term<L, R>(L::opp(i), wall, dst, qs));
+                    S::store(fd + L::opp(i) * qs + nd, v_add(f[i], wall_term<L, R>(L::opp(i), wall, dst, qs)));
                 } else {
                     S::store(fd + i * qs + dst, f[i]);
                 }
@@ -225,20 +226,32 @@ struct StepKernel {
     }
 };
 
-// Bulk: interior nodes (kind 0) of tile (blockIdx.x, blockIdx.y) of plane
-// blockIdx.z. Every other non-solid node is in the special list.
+// One node of the bulk grid. Every lane of the warp calls it (in = false
+// for lanes past the edge of the domain), because the path is chosen per
+// warp: a warp whose nodes are all interior (kind 0) takes the branch-free
+// path; in any other warp every lane takes the general path (interior lanes
+// with an empty mask), so no warp runs both paths one after the other.
+// Solid nodes are skipped, SPECIAL nodes are left to the boundary warps.
+template <class L, int ST, int VAR>
+__device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z, int64_t nd, bool in)
+{
+    using K = StepKernel<L, ST, VAR>;
+    const uint8_t k = in ? a.kind[nd] : KIND_SOLID;
+    if (__all_sync(0xffffffffu, !in || k == KIND_FLUID)) {
+        if (in) K::interior(a, nd);
+    } else if (!(k & (KIND_SOLID | KIND_SPECIAL))) {
+        K::template node<false>(a, x, y, z, nd, a.nbr[nd], -1);
+    }
+}
+
+// Bulk: tile (blockIdx.x, blockIdx.y) of plane z; tile_x is a multiple of
+// 32, so every warp lies in one row.
 template <class L, int ST, int VAR>
 __device__ __forceinline__ void bulk_tile(const StepArgs& a, int z)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= a.nx || y >= a.ny) return;
-    const int64_t nd = ((int64_t)z * a.ny + y) * a.pitch + x;
-    const uint8_t k = a.kind[nd];
-    if (k == KIND_FLUID)
-        StepKernel<L, ST, VAR>::interior(a, nd);
-    else if (!(k & (KIND_SOLID | KIND_SPECIAL)))
-        StepKernel<L, ST, VAR>::template node<false>(a, x, y, z, nd, a.nbr[nd], -1);
+    bulk_node<L, ST, VAR>(a, x, y, z, ((int64_t)z * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny);
 }
 
 template <class L, int ST, int VAR>
