@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -45,7 +45,7 @@ class Grid(C.Structure):
 class Physics(C.Structure):
     _fields_ = [
         ("omega_plus", C.c_double), ("omega_minus", C.c_double), ("force", C.c_double * 3),
-        ("wall_u", vp), ("force_field", vp), ("solid_nbr", vp),
+        ("wall_u", vp), ("force_field", vp), ("solid_nbr", vp), ("round_seed", vp),
     ]
 
 
@@ -89,6 +89,7 @@ class Batch(C.Structure):
     _fields_ = [
         ("lattice", i32), ("storage", i32), ("n_domains", i32), ("domains", vp), ("n_tiles", i32), ("tiles", vp),
         ("tile_x", i32), ("tile_y", i32), ("blocks", i32), ("kind", vp), ("solid_nbr", vp), ("wall_u", vp),
+        ("round_seed", vp),
     ]
 
 

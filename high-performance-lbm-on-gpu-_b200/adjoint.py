@@ -71,6 +71,8 @@ class AdjointRun:
         params, d_rules = self.make_params(scale)
         if params.immersed is not None:
             raise ValueError("the adjoint supports walls, forces and link rules (no immersed bodies)")
+        if params.dtype not in ("float32", "float64"):
+            raise ValueError("the adjoint needs float32 or float64 storage (its recomputed forward must be exact)")
         s = CudaSolver(params, variant="pull", block=self.block, force_field=G, graph=False, keep_zero_terms=True)
         self.solver, self.params, self.d_rules = s, params, d_rules
         torch = s.torch

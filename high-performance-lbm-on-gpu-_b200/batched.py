@@ -95,6 +95,9 @@ class BatchedSolver:
         self.total = off
         self._f = torch.zeros(off, dtype=self.t_store, device=self.device)
         self._g = torch.zeros(off, dtype=self.t_store, device=self.device)
+        # step counter (two slots) of the stochastic rounding of 16-bit storage,
+        # shared by all domains (they advance together); reset by initialize
+        self._seed = torch.zeros(2, dtype=torch.int32, device=self.device)
         self._kind = torch.full((koff,), N.KIND_SOLID, dtype=torch.uint8, device=self.device)
         self._wall = None
         if walls:
@@ -161,6 +164,7 @@ class BatchedSolver:
         self.batch = N.Batch(
             self.grids[0].lattice, self.grids[0].storage, len(self.params), N.ptr(self._domains), len(tiles),
             N.ptr(self._tiles), bx, by, self.blocks, N.ptr(self._kind), N.ptr(self._nbr), N.ptr(self._wall),
+            N.ptr(self._seed),
         )
         self._graphs.clear()
 
@@ -180,7 +184,8 @@ class BatchedSolver:
         wall = None
         if self.wall_offsets[i] >= 0:
             wall = self._wall[self.wall_offsets[i] :]
-        return N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(wall), None, N.ptr(self._nbr[self.kind_offsets[i]:]))
+        return N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(wall), None, N.ptr(self._nbr[self.kind_offsets[i]:]),
+                         N.ptr(self._seed))
 
     # ------------------------------------------------------------------ state
     def initialize(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0, domain: int | None = None) -> None:
@@ -202,6 +207,7 @@ class BatchedSolver:
             N.call("lbm_init_equilibrium", N.C.byref(g), N.C.byref(ph), N.ptr(rho_t), N.ptr(u_t), N.LAYOUT_PULL,
                    N.ptr(self._slice(self._f, i)), stream)
         self._g.copy_(self._f)
+        self._seed.zero_()
         self._graphs.clear()
         self.time_step = 0
 

@@ -62,6 +62,11 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
     a.force_field = p->force_field;
     a.nbr = p->solid_nbr;
     if (!a.nbr) return LBM_ERR_INVALID;
+    // 16-bit storage rounds stochastically and needs the step counter
+    const bool half = g->storage == LBM_F16 || g->storage == LBM_BF16;
+    if (half && !p->round_seed) return LBM_ERR_INVALID;
+    a.seed = half ? p->round_seed : nullptr;
+    a.parity = 0;
     if (sp)
         a.sp = *sp;
     else
@@ -85,6 +90,7 @@ extern "C" int lbm_step_pull(const lbm_grid_t* g, const lbm_physics_t* p, const 
     int tx = 0, ty = 0, mode = 0;
     int st = make_args(a, g, p, sp, launch, kind, f_src, f_dst, tx, ty, mode);
     if (st != LBM_OK) return st;
+    a.parity = (uintptr_t)f_src > (uintptr_t)f_dst ? 1 : 0;
     const int lattice = g->lattice, storage = g->storage;
     auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, LBM_PULL, mode, tx, ty, (cudaStream_t)stream); };
     return record(run());
@@ -100,6 +106,7 @@ extern "C" int lbm_step_aa(const lbm_grid_t* g, const lbm_physics_t* p, const lb
     int tx = 0, ty = 0, mode = 0;
     int st = make_args(a, g, p, sp, launch, kind, f, f, tx, ty, mode);
     if (st != LBM_OK) return st;
+    a.parity = parity == LBM_AA_ODD ? 1 : 0;
     const int lattice = g->lattice, storage = g->storage;
     auto run = [&]() -> int { LBM_DISPATCH(lattice, storage, step_dispatch, a, parity, mode, tx, ty, (cudaStream_t)stream); };
     return record(run());
@@ -120,4 +127,4 @@ extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t wh
 
 extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
 
-extern "C" int32_t lbm_abi_version(void) { return 1; }
+extern "C" int32_t lbm_abi_version(void) { return 2; }

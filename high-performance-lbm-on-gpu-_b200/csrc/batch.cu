@@ -21,6 +21,8 @@ struct BatchArgs {
     const void* wall;
     const void* f_src;
     void* f_dst;
+    uint32_t* seed;  // step counter of the stochastic rounding (16-bit storage)
+    int parity;
 };
 
 template <int ST>
@@ -46,12 +48,16 @@ __device__ __forceinline__ StepArgs domain_args(const BatchArgs& b, int d)
     a.f_dst = static_cast<T*>(b.f_dst) + D.offset;
     a.wall_u = (b.wall != nullptr && D.wall_offset >= 0) ? static_cast<const R*>(b.wall) + D.wall_offset : nullptr;
     a.force_field = nullptr;
+    a.seed = b.seed;
+    a.parity = b.parity;
     return a;
 }
 
 template <class L, int ST>
 __global__ void __launch_bounds__(256, 1) lbm_batch_kernel(const BatchArgs b)
 {
+    if (b.seed != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+        b.seed[b.parity ^ 1] = b.seed[b.parity] + 1u;
     for (int item = blockIdx.x; item < b.n_tiles; item += gridDim.x) {
         const int4 t = b.tiles[item];
         const StepArgs a = domain_args<ST>(b, t.x);
@@ -73,6 +79,8 @@ int batch_step(const lbm_batch_t& bt, const void* src, void* dst, cudaStream_t s
     b.wall = bt.wall_u;
     b.f_src = src;
     b.f_dst = dst;
+    b.seed = (bt.storage == LBM_F16 || bt.storage == LBM_BF16) ? bt.round_seed : nullptr;
+    b.parity = (uintptr_t)src > (uintptr_t)dst ? 1 : 0;
     lbm_batch_kernel<L, ST><<<bt.blocks, dim3(bt.tile_x, bt.tile_y), 0, s>>>(b);
     return launch_status();
 }
@@ -98,6 +106,7 @@ extern "C" int lbm_batch_step(const lbm_batch_t* bt, const void* f_src, void* f_
     if (bt->n_tiles < 0 || (bt->n_tiles > 0 && !bt->tiles)) return LBM_ERR_INVALID;
     if (bt->tile_x <= 0 || bt->tile_y <= 0 || bt->tile_x % 32 || bt->tile_x * bt->tile_y > 256 || bt->blocks <= 0)
         return LBM_ERR_INVALID;
+    if ((bt->storage == LBM_F16 || bt->storage == LBM_BF16) && !bt->round_seed) return LBM_ERR_INVALID;
     LBM_DISPATCH(bt->lattice, bt->storage, batch_step, *bt, f_src, f_dst, (cudaStream_t)stream);
 }
 

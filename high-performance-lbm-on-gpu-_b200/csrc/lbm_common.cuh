@@ -60,6 +60,36 @@ struct D3Q19 {
     __host__ __device__ static constexpr double w(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }
 };
 
+// ---------------------------------------------------------------- stochastic rounding
+// The step kernels store post-collision populations in 16-bit formats with
+// stochastic rounding: a value between two neighbouring 16-bit numbers goes
+// to the upper one with probability equal to its distance from the lower one
+// (in units of their gap). Rounding then adds no bias, and a per-step change
+// smaller than half a gap still accumulates; round-to-nearest drops such
+// changes every step, which stalls slow or weakly forced flows.
+// The random bits are a pure function of (node, step, direction), so runs are
+// reproducible and the oracle replays them bit for bit:
+//   h   = lowbias32(node ^ lowbias32(step)),   node = x + nx (y + ny z)
+//   r_i = (h * sr_mult(i)) >> (32 - dropped bits)
+// lowbias32 is the 32-bit integer hash published by C. Wellons
+// (hash-prospector); the odd multipliers decorrelate the directions.
+__host__ __device__ constexpr uint32_t sr_mult(int i) { return 0x9E3779B9u * (uint32_t)(2 * i + 1); }
+
+__host__ __device__ __forceinline__ uint32_t lowbias32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t sr_node_hash(int64_t natural, uint32_t step)
+{
+    return lowbias32((uint32_t)natural ^ lowbias32(step));
+}
+
 // ---------------------------------------------------------------- storage
 // Populations are stored shifted (f~ = f - w). Float16 storage multiplies by
 // a power of two before rounding so that small f~ stay out of the subnormal
@@ -72,10 +102,13 @@ template <int ST> struct Storage;
 template <> struct Storage<LBM_F32> {
     using T = float;
     using R = float;
+    static constexpr bool STOCHASTIC = false;
     __device__ static __forceinline__ R load(const T* p) { return *p; }
     __device__ static __forceinline__ R load_nc(const T* p) { return __ldg(p); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = v; }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t, int) { *p = v; }
     __device__ static __forceinline__ R round(R v) { return v; }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t, int) { return v; }
     __device__ static __forceinline__ T encode(R v) { return v; }
     __device__ static __forceinline__ R decode(T v) { return v; }
 };
@@ -83,10 +116,13 @@ template <> struct Storage<LBM_F32> {
 template <> struct Storage<LBM_F64> {
     using T = double;
     using R = double;
+    static constexpr bool STOCHASTIC = false;
     __device__ static __forceinline__ R load(const T* p) { return *p; }
     __device__ static __forceinline__ R load_nc(const T* p) { return __ldg(p); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = v; }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t, int) { *p = v; }
     __device__ static __forceinline__ R round(R v) { return v; }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t, int) { return v; }
     __device__ static __forceinline__ T encode(R v) { return v; }
     __device__ static __forceinline__ R decode(T v) { return v; }
 };
@@ -96,10 +132,20 @@ template <> struct Storage<LBM_F16> {
     using R = float;
     __device__ static __forceinline__ R decode(T v) { return __half2float(v) * FP16_INV_SCALE; }
     __device__ static __forceinline__ T encode(R v) { return __float2half_rn(v * FP16_SCALE); }
+    // stochastic: add 13 random bits below the 10 kept mantissa bits of the
+    // scaled float32, then truncate (exact in the normal float16 range)
+    __device__ static __forceinline__ T encode_sr(R v, uint32_t h, int i)
+    {
+        const uint32_t b = __float_as_uint(v * FP16_SCALE) + ((h * sr_mult(i)) >> 19);
+        return __float2half_rn(__uint_as_float(b & 0xFFFFE000u));
+    }
+    static constexpr bool STOCHASTIC = true;
     __device__ static __forceinline__ R load(const T* p) { return decode(*p); }
     __device__ static __forceinline__ R load_nc(const T* p) { return decode(__ldg(p)); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = encode(v); }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t h, int i) { *p = encode_sr(v, h, i); }
     __device__ static __forceinline__ R round(R v) { return decode(encode(v)); }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t h, int i) { return decode(encode_sr(v, h, i)); }
 };
 
 template <> struct Storage<LBM_BF16> {
@@ -107,10 +153,19 @@ template <> struct Storage<LBM_BF16> {
     using R = float;
     __device__ static __forceinline__ R decode(T v) { return __bfloat162float(v); }
     __device__ static __forceinline__ T encode(R v) { return __float2bfloat16_rn(v); }
+    // stochastic: add 16 random bits below the kept half, then truncate
+    __device__ static __forceinline__ T encode_sr(R v, uint32_t h, int i)
+    {
+        const uint32_t b = __float_as_uint(v) + ((h * sr_mult(i)) >> 16);
+        return __ushort_as_bfloat16((unsigned short)(b >> 16));
+    }
+    static constexpr bool STOCHASTIC = true;
     __device__ static __forceinline__ R load(const T* p) { return decode(*p); }
     __device__ static __forceinline__ R load_nc(const T* p) { return decode(__ldg(p)); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = encode(v); }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t h, int i) { *p = encode_sr(v, h, i); }
     __device__ static __forceinline__ R round(R v) { return decode(encode(v)); }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t h, int i) { return decode(encode_sr(v, h, i)); }
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -239,7 +294,20 @@ struct StepArgs {
     const void* wall_u;
     const void* force_field;
     const uint32_t* nbr;  // solid-neighbour mask per node
+    // Step counter of the stochastic rounding (16-bit storage): the launch
+    // reads seed[parity] and its bulk part writes seed[parity ^ 1] = +1.
+    uint32_t* seed;
+    int parity;
     lbm_special_t sp;
 };
+
+// The bulk (or fused) launch of a step advances the step counter: one thread
+// writes the other slot, which no thread of this step reads.
+__device__ __forceinline__ void advance_seed(const StepArgs& a)
+{
+    if (a.seed != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
+        threadIdx.y == 0)
+        a.seed[a.parity ^ 1] = a.seed[a.parity] + 1u;
+}
 
 }  // namespace lbm

@@ -65,7 +65,7 @@ struct StepKernel {
     // the same for all threads (-c_i . strides), so the compiler keeps them in
     // uniform registers and each access is [thread pointer + uniform offset].
     // All Q loads are independent and issued back to back.
-    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd)
+    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd, int64_t natural)
     {
         const int64_t qs = a.qstride;
         const int64_t py = a.pitch;
@@ -90,16 +90,17 @@ struct StepKernel {
             if (L::D == 3) Fz += ff[2 * qs + nd];
         }
         collide<L, R>(f, R(a.wp), R(a.wm), Fx, Fy, Fz);
+        const uint32_t h = S::STOCHASTIC ? sr_node_hash(natural, a.seed[a.parity]) : 0u;
         T* fd = static_cast<T*>(a.f_dst) + nd;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const int64_t shift = L::cx(i) + L::cy(i) * py + L::cz(i) * pz;
             if (VAR == LBM_PULL)
-                S::store(fd + i * qs, f[i]);
+                S::store_sr(fd + i * qs, f[i], h, i);
             else if (VAR == LBM_AA_EVEN)
-                S::store(fd + L::opp(i) * qs, f[i]);
+                S::store_sr(fd + L::opp(i) * qs, f[i], h, i);
             else
-                S::store(fd + (i * qs + shift), f[i]);
+                S::store_sr(fd + (i * qs + shift), f[i], h, i);
         }
     }
 
@@ -181,15 +182,16 @@ struct StepKernel {
             }
         }
         collide<L, R>(f, R(a.wp), R(a.wm), Fx, Fy, Fz);
+        const uint32_t h = S::STOCHASTIC ? sr_node_hash(((int64_t)z * a.ny + y) * a.nx + x, a.seed[a.parity]) : 0u;
 
-        // ---- store
+        // ---- store (16-bit formats: stochastic rounding, see sr_node_hash)
         T* fd = static_cast<T*>(a.f_dst);
         if (VAR == LBM_PULL) {
 #pragma unroll
-            for (int i = 0; i < Q; ++i) S::store(fd + i * qs + nd, f[i]);
+            for (int i = 0; i < Q; ++i) S::store_sr(fd + i * qs + nd, f[i], h, i);
         } else if (VAR == LBM_AA_EVEN) {
 #pragma unroll
-            for (int i = 0; i < Q; ++i) S::store(fd + L::opp(i) * qs + nd, f[i]);
+            for (int i = 0; i < Q; ++i) S::store_sr(fd + L::opp(i) * qs + nd, f[i], h, i);
         } else {
 #pragma unroll
             for (int i = 0; i < Q; ++i) {
@@ -198,9 +200,9 @@ struct StepKernel {
                 const int dz = L::cz(i) > 0 ? zp : (L::cz(i) < 0 ? zm : z);
                 const int64_t dst = ((int64_t)dz * a.ny + dy) * a.pitch + dx;
                 if (i != 0 && ((bb >> L::opp(i)) & 1u)) {
-                    S::store(fd + L::opp(i) * qs + nd, v_add(f[i], wall_term<L, R>(L::opp(i), wall, dst, qs)));
+                    S::store_sr(fd + L::opp(i) * qs + nd, v_add(f[i], wall_term<L, R>(L::opp(i), wall, dst, qs)), h, i);
                 } else {
-                    S::store(fd + i * qs + dst, f[i]);
+                    S::store_sr(fd + i * qs + dst, f[i], h, i);
                 }
             }
         }
@@ -219,7 +221,7 @@ struct StepKernel {
 #pragma unroll
                     for (int j = 1; j < Q; ++j)
                         if (j == k) v = f[j];
-                    out[e++] = S::round(v);
+                    out[e++] = S::round_sr(v, h, k);
                 }
             }
         }
@@ -238,7 +240,7 @@ __device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z
     using K = StepKernel<L, ST, VAR>;
     const uint8_t k = in ? a.kind[nd] : KIND_SOLID;
     if (__all_sync(0xffffffffu, !in || k == KIND_FLUID)) {
-        if (in) K::interior(a, nd);
+        if (in) K::interior(a, nd, ((int64_t)z * a.ny + y) * a.nx + x);
     } else if (!(k & (KIND_SOLID | KIND_SPECIAL))) {
         K::template node<false>(a, x, y, z, nd, a.nbr[nd], -1);
     }
@@ -271,6 +273,7 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
 template <class L, int ST, int VAR>
 __global__ void __launch_bounds__(256) lbm_bulk_kernel(const StepArgs a)
 {
+    advance_seed(a);
     bulk_tile<L, ST, VAR>(a, blockIdx.z);
 }
 
@@ -286,6 +289,7 @@ __global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
     }
     const int z = blockIdx.z;
     if (z < a.nz) {
+        advance_seed(a);
         bulk_tile<L, ST, VAR>(a, z);
     } else {
         const int64_t b = ((int64_t)(z - a.nz) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;

@@ -226,6 +226,10 @@ class CudaSolver(Solver):
         if force_field is not None:
             self._force_field = self._upload_field(np.asarray(force_field, dtype=np.float64).reshape(d, *shape))
         self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field), None)
+        # step counter (two slots) of the stochastic rounding of 16-bit storage;
+        # reset whenever the populations are set
+        self._seed = torch.zeros(2, dtype=torch.int32, device=self.device)
+        self.physics.round_seed = N.ptr(self._seed)
 
         # ---- immersed boundary and link rules -> special nodes
         self._ibm = None
@@ -458,6 +462,7 @@ class CudaSolver(Solver):
         self._after_state_change()
 
     def _after_state_change(self):
+        self._seed.zero_()
         s = self._special
         if self.variant == "aa" and s.n_export:
             self._export_cur = s.tensors["export_a"]

@@ -63,6 +63,12 @@ typedef struct lbm_physics {
     const void* force_field; /* real[d][qstride] per-node body force added to force[], or NULL */
     const uint32_t* solid_nbr; /* per node: bit i set where x - c_i is solid (lbm_classify); read only
                                   at fluid nodes that are not interior */
+    uint32_t* round_seed;  /* float16/bfloat16 storage (required there, ignored otherwise): two uint32
+                              slots holding the step counter of the stochastic rounding of stored
+                              populations. A step reads slot p and its bulk (or fused) launch writes
+                              slot 1 - p with the count + 1, where p = (f_src > f_dst) for
+                              lbm_step_pull and p = parity for lbm_step_aa. Set both slots to the same
+                              value (0) whenever the populations are set. */
 } lbm_physics_t;
 
 /* Nodes updated by the boundary warps, and the link rules they apply.
@@ -320,6 +326,7 @@ typedef struct lbm_batch {
     const uint8_t* kind;           /* kind pool (domain i at kind_offset) */
     const uint32_t* solid_nbr;     /* solid-neighbour pool, same offsets as kind */
     const void* wall_u;            /* wall pool (compute type) or NULL */
+    uint32_t* round_seed;          /* as lbm_physics_t.round_seed, one counter for the whole batch */
 } lbm_batch_t;
 
 /* One two-lattice pull step of every domain of the batch -- the batched

@@ -16,6 +16,8 @@ from .lbm_oracle import (  # noqa: F401
     OracleSolver,
     collide,
     equilibrium,
+    lowbias32,
     quantize,
+    stochastic_round,
     stream_pull,
 )

@@ -7,7 +7,9 @@ simulation dtype so float32 runs round like the reference's float32 runs.
 16-bit storage ("float16", "bfloat16") has no counterpart in the reference.
 The oracle emulates it: arithmetic in float32, populations rounded to the
 storage format after every step exactly as the CUDA kernels store them
-(``quantize``), so the GPU path can be checked bit-for-tolerance.
+(``stochastic_round``: the same hash of node, step and direction, so the
+rounding decisions are replayed bit for bit; the initial state is rounded to
+nearest, ``quantize``), so the GPU path can be checked bit-for-tolerance.
 """
 
 from __future__ import annotations
@@ -39,6 +41,50 @@ def quantize(f: np.ndarray, dtype: str) -> np.ndarray:
         rounded = ((bits + bias) & 0xFFFF0000).astype(np.uint32)
         return rounded.view(np.float32)
     return f
+
+
+SR_GOLDEN = 0x9E3779B9
+
+
+def lowbias32(x):
+    """32-bit integer hash "lowbias32" of C. Wellons' hash-prospector (uint32 in, uint32 out)."""
+    x = np.asarray(x, dtype=np.uint32).copy()
+    x ^= x >> np.uint32(16)
+    x *= np.uint32(0x7FEB352D)
+    x ^= x >> np.uint32(15)
+    x *= np.uint32(0x846CA68B)
+    x ^= x >> np.uint32(16)
+    return x
+
+
+def stochastic_round(f: np.ndarray, dtype: str, step: int) -> np.ndarray:
+    """Stochastic rounding of post-collision populations to 16-bit storage, as the step kernels store them.
+
+    f has shape (q, *shape) in natural order. For node n (flat index) at
+    step t: h = lowbias32(n ^ lowbias32(t)); direction i adds the top 13
+    (float16, after the 2^14 scale) or 16 (bfloat16) bits of h * (golden *
+    (2i + 1)) mod 2^32 below the kept mantissa bits, then truncates.
+    float32/float64 storage is returned unchanged.
+    """
+    if dtype not in ("float16", "bfloat16"):
+        return f
+    q = f.shape[0]
+    flat = f.reshape(q, -1)
+    node = np.arange(flat.shape[1], dtype=np.uint64).astype(np.uint32)
+    h = lowbias32(node ^ lowbias32(np.uint32(step & 0xFFFFFFFF)))
+    out = np.empty(flat.shape, dtype=np.float32)
+    with np.errstate(over="ignore"):
+        for i in range(q):
+            mult = np.uint32((SR_GOLDEN * (2 * i + 1)) & 0xFFFFFFFF)
+            x = flat[i].astype(np.float32)
+            if dtype == "float16":
+                x = x * np.float32(FP16_SCALE)
+                bits = (x.view(np.uint32) + ((h * mult) >> np.uint32(19))) & np.uint32(0xFFFFE000)
+                out[i] = bits.view(np.float32).astype(np.float16).astype(np.float32) * np.float32(1.0 / FP16_SCALE)
+            else:
+                bits = (x.view(np.uint32) + ((h * mult) >> np.uint32(16))) & np.uint32(0xFFFF0000)
+                out[i] = bits.view(np.float32)
+    return out.reshape(f.shape)
 
 
 def _dot(c, vec):
@@ -226,9 +272,11 @@ class OracleSolver:
         f = equilibrium(self.lattice, drho, tuple(np.asarray(a, dtype=self.cdt) for a in u))
         self.f = quantize(f, self.dtype)
         self.time_step = 0
+        self.round_step = 0
 
     def set_populations(self, f):
         self.f = np.array(f, dtype=self.cdt, copy=True)
+        self.round_step = 0
 
     def _force_components(self, dt):
         """Uniform force, plus the per-node extension field (not the IBM field)."""
@@ -261,7 +309,8 @@ class OracleSolver:
             values = const + (coeff * f.reshape(-1)[slots]).sum(axis=1)
             streamed.reshape(-1)[target] = values
         post = collide(lattice, streamed, self.rates[0], self.rates[1], force)
-        self.f = quantize(np.where(self.fluid, post, f), self.dtype)
+        self.f = stochastic_round(np.where(self.fluid, post, f), self.dtype, self.round_step)
+        self.round_step += 1
 
     def run(self, steps, check_every=500):
         done = 0
