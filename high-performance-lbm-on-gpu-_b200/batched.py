@@ -97,7 +97,7 @@ class BatchedSolver:
         self._g = torch.zeros(off, dtype=self.t_store, device=self.device)
         # step counter (two slots) of the stochastic rounding of 16-bit storage,
         # shared by all domains (they advance together); reset by initialize
-        self._seed = torch.zeros(2, dtype=torch.int32, device=self.device)
+        self._seed = torch.zeros(4, dtype=torch.int32, device=self.device)
         self._kind = torch.full((koff,), N.KIND_SOLID, dtype=torch.uint8, device=self.device)
         self._wall = None
         if walls:
@@ -207,7 +207,7 @@ class BatchedSolver:
             N.call("lbm_init_equilibrium", N.C.byref(g), N.C.byref(ph), N.ptr(rho_t), N.ptr(u_t), N.LAYOUT_PULL,
                    N.ptr(self._slice(self._f, i)), stream)
         self._g.copy_(self._f)
-        self._seed.zero_()
+        self._seed[:2].zero_()
         self._graphs.clear()
         self.time_step = 0
 

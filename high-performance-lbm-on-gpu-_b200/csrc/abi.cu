@@ -71,6 +71,15 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
         a.sp = *sp;
     else
         memset(&a.sp, 0, sizeof(a.sp));
+    // collision constants, computed once per launch
+    a.guo_const = true;
+    if (g->lattice == LBM_D2Q9) {
+        relax_constants<D2Q9, float>(a.rf, a.wp, a.wm, a.fx, a.fy, a.fz);
+        relax_constants<D2Q9, double>(a.rd, a.wp, a.wm, a.fx, a.fy, a.fz);
+    } else {
+        relax_constants<D3Q19, float>(a.rf, a.wp, a.wm, a.fx, a.fy, a.fz);
+        relax_constants<D3Q19, double>(a.rd, a.wp, a.wm, a.fx, a.fy, a.fz);
+    }
     return LBM_OK;
 }
 

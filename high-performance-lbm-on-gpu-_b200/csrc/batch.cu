@@ -25,7 +25,7 @@ struct BatchArgs {
     int parity;
 };
 
-template <int ST>
+template <class L, int ST>
 __device__ __forceinline__ StepArgs domain_args(const BatchArgs& b, int d)
 {
     const lbm_domain_t& D = b.domains[d];
@@ -50,6 +50,12 @@ __device__ __forceinline__ StepArgs domain_args(const BatchArgs& b, int d)
     a.force_field = nullptr;
     a.seed = b.seed;
     a.parity = b.parity;
+    // collision scalars per tile; force terms per node (no per-domain tables)
+    a.guo_const = false;
+    if constexpr (ST == LBM_F64)
+        relax_scalars<L, double>(a.rd, D.omega_plus, D.omega_minus);
+    else
+        relax_scalars<L, float>(a.rf, D.omega_plus, D.omega_minus);
     return a;
 }
 
@@ -60,7 +66,7 @@ __global__ void __launch_bounds__(256, 1) lbm_batch_kernel(const BatchArgs b)
         b.seed[b.parity ^ 1] = b.seed[b.parity] + 1u;
     for (int item = blockIdx.x; item < b.n_tiles; item += gridDim.x) {
         const int4 t = b.tiles[item];
-        const StepArgs a = domain_args<ST>(b, t.x);
+        const StepArgs a = domain_args<L, ST>(b, t.x);
         const int x = t.y * blockDim.x + threadIdx.x;
         const int y = t.z * blockDim.y + threadIdx.y;
         bulk_node<L, ST, LBM_PULL>(a, x, y, t.w, ((int64_t)t.w * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny);

@@ -67,15 +67,20 @@ struct D3Q19 {
 // (in units of their gap). Rounding then adds no bias, and a per-step change
 // smaller than half a gap still accumulates; round-to-nearest drops such
 // changes every step, which stalls slow or weakly forced flows.
-// The random bits are a pure function of (node, step, direction), so runs are
-// reproducible and the oracle replays them bit for bit:
-//   h   = lowbias32(node ^ lowbias32(step)),   node = x + nx (y + ny z)
-//   r_i = (h * sr_mult(i)) >> (32 - dropped bits)
-// lowbias32 is the 32-bit integer hash published by C. Wellons
-// (hash-prospector); the odd multipliers decorrelate the directions.
-__host__ __device__ constexpr uint32_t sr_mult(int i) { return 0x9E3779B9u * (uint32_t)(2 * i + 1); }
-
-__host__ __device__ __forceinline__ uint32_t lowbias32(uint32_t x)
+// The rounding is Blackwell's cvt.rs: a float32 v goes to the 16-bit format
+// by adding R units of 2^-13 (float16; 2^-16 for bfloat16) of the
+// destination spacing at |v| to |v| and truncating toward zero; float16
+// magnitudes that reach 65536 become infinite. One instruction converts two
+// values, taking R from bits 0-12 (0-15) of a 32-bit random word for the
+// lower half and bits 16-28 (16-31) for the upper half. Nodes pair up along x
+// (x even with x + 1) and share one word per direction:
+//   pair = (z ny + y) ceil(nx / 2) + floor(x / 2),  h = lowbias32(pair ^ lowbias32(step))
+//   word_i = (h ^ K_i) * 0x9E3779B9,  K_i = lowbias32(i + 1)
+// the even node taking the lower half's bits, the odd node the upper half's.
+// It is a pure function of (node, step, direction): runs are reproducible and
+// the oracle replays them bit for bit. lowbias32 is the 32-bit integer hash
+// published by C. Wellons (hash-prospector).
+__host__ __device__ constexpr uint32_t lowbias32(uint32_t x)
 {
     x ^= x >> 16;
     x *= 0x7feb352du;
@@ -85,9 +90,31 @@ __host__ __device__ __forceinline__ uint32_t lowbias32(uint32_t x)
     return x;
 }
 
-__device__ __forceinline__ uint32_t sr_node_hash(int64_t natural, uint32_t step)
+__host__ __device__ constexpr uint32_t sr_key(int i) { return lowbias32((uint32_t)i + 1u); }
+constexpr uint32_t SR_MULT = 0x9E3779B9u;
+
+__device__ __forceinline__ int64_t sr_pair(int nx, int ny, int x, int y, int z)
 {
-    return lowbias32((uint32_t)natural ^ lowbias32(step));
+    return ((int64_t)z * ny + y) * ((nx + 1) >> 1) + (x >> 1);
+}
+__device__ __forceinline__ uint32_t sr_pair_hash(int64_t pair, uint32_t step)
+{
+    return lowbias32((uint32_t)pair ^ lowbias32(step));
+}
+__device__ __forceinline__ uint32_t sr_word(uint32_t h, int i) { return (h ^ sr_key(i)) * SR_MULT; }
+
+// d = (16-bit hi : 16-bit lo), stochastically rounded with rbits
+__device__ __forceinline__ uint32_t cvt_rs_f16x2(float hi, float lo, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+__device__ __forceinline__ uint32_t cvt_rs_bf16x2(float hi, float lo, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
 }
 
 // ---------------------------------------------------------------- storage
@@ -103,12 +130,13 @@ template <> struct Storage<LBM_F32> {
     using T = float;
     using R = float;
     static constexpr bool STOCHASTIC = false;
+    static constexpr int SCALE_LOG2 = 0;
     __device__ static __forceinline__ R load(const T* p) { return *p; }
     __device__ static __forceinline__ R load_nc(const T* p) { return __ldg(p); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = v; }
-    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t, int) { *p = v; }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t, int, bool) { *p = v; }
     __device__ static __forceinline__ R round(R v) { return v; }
-    __device__ static __forceinline__ R round_sr(R v, uint32_t, int) { return v; }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t, int, bool) { return v; }
     __device__ static __forceinline__ T encode(R v) { return v; }
     __device__ static __forceinline__ R decode(T v) { return v; }
 };
@@ -117,12 +145,13 @@ template <> struct Storage<LBM_F64> {
     using T = double;
     using R = double;
     static constexpr bool STOCHASTIC = false;
+    static constexpr int SCALE_LOG2 = 0;
     __device__ static __forceinline__ R load(const T* p) { return *p; }
     __device__ static __forceinline__ R load_nc(const T* p) { return __ldg(p); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = v; }
-    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t, int) { *p = v; }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t, int, bool) { *p = v; }
     __device__ static __forceinline__ R round(R v) { return v; }
-    __device__ static __forceinline__ R round_sr(R v, uint32_t, int) { return v; }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t, int, bool) { return v; }
     __device__ static __forceinline__ T encode(R v) { return v; }
     __device__ static __forceinline__ R decode(T v) { return v; }
 };
@@ -132,20 +161,26 @@ template <> struct Storage<LBM_F16> {
     using R = float;
     __device__ static __forceinline__ R decode(T v) { return __half2float(v) * FP16_INV_SCALE; }
     __device__ static __forceinline__ T encode(R v) { return __float2half_rn(v * FP16_SCALE); }
-    // stochastic: add 13 random bits below the 10 kept mantissa bits of the
-    // scaled float32, then truncate (exact in the normal float16 range)
-    __device__ static __forceinline__ T encode_sr(R v, uint32_t h, int i)
+    // stochastic rounding of one value; hi: the odd node of its pair
+    __device__ static __forceinline__ T encode_sr(R v, uint32_t h, int i, bool hi)
     {
-        const uint32_t b = __float_as_uint(v * FP16_SCALE) + ((h * sr_mult(i)) >> 19);
-        return __float2half_rn(__uint_as_float(b & 0xFFFFE000u));
+        const float s = v * FP16_SCALE;
+        const uint32_t w = cvt_rs_f16x2(s, s, sr_word(h, i));
+        return __ushort_as_half((unsigned short)(hi ? w >> 16 : w));
     }
     static constexpr bool STOCHASTIC = true;
     __device__ static __forceinline__ R load(const T* p) { return decode(*p); }
     __device__ static __forceinline__ R load_nc(const T* p) { return decode(__ldg(p)); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = encode(v); }
-    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t h, int i) { *p = encode_sr(v, h, i); }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t h, int i, bool hi) { *p = encode_sr(v, h, i, hi); }
     __device__ static __forceinline__ R round(R v) { return decode(encode(v)); }
-    __device__ static __forceinline__ R round_sr(R v, uint32_t h, int i) { return decode(encode_sr(v, h, i)); }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t h, int i, bool hi) { return decode(encode_sr(v, h, i, hi)); }
+    // The vector kernel computes on populations times 2^14 (collide with
+    // SCALE_LOG2 = 14), so its conversions need no multiply.
+    static constexpr int SCALE_LOG2 = 14;
+    __device__ static __forceinline__ R decode_lo(uint32_t w) { return __low2float(*reinterpret_cast<const __half2*>(&w)); }
+    __device__ static __forceinline__ R decode_hi(uint32_t w) { return __high2float(*reinterpret_cast<const __half2*>(&w)); }
+    __device__ static __forceinline__ uint32_t pack_sr(R lo, R hi, uint32_t rbits) { return cvt_rs_f16x2(hi, lo, rbits); }
 };
 
 template <> struct Storage<LBM_BF16> {
@@ -153,19 +188,22 @@ template <> struct Storage<LBM_BF16> {
     using R = float;
     __device__ static __forceinline__ R decode(T v) { return __bfloat162float(v); }
     __device__ static __forceinline__ T encode(R v) { return __float2bfloat16_rn(v); }
-    // stochastic: add 16 random bits below the kept half, then truncate
-    __device__ static __forceinline__ T encode_sr(R v, uint32_t h, int i)
+    __device__ static __forceinline__ T encode_sr(R v, uint32_t h, int i, bool hi)
     {
-        const uint32_t b = __float_as_uint(v) + ((h * sr_mult(i)) >> 16);
-        return __ushort_as_bfloat16((unsigned short)(b >> 16));
+        const uint32_t w = cvt_rs_bf16x2(v, v, sr_word(h, i));
+        return __ushort_as_bfloat16((unsigned short)(hi ? w >> 16 : w));
     }
     static constexpr bool STOCHASTIC = true;
     __device__ static __forceinline__ R load(const T* p) { return decode(*p); }
     __device__ static __forceinline__ R load_nc(const T* p) { return decode(__ldg(p)); }
     __device__ static __forceinline__ void store(T* p, R v) { *p = encode(v); }
-    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t h, int i) { *p = encode_sr(v, h, i); }
+    __device__ static __forceinline__ void store_sr(T* p, R v, uint32_t h, int i, bool hi) { *p = encode_sr(v, h, i, hi); }
     __device__ static __forceinline__ R round(R v) { return decode(encode(v)); }
-    __device__ static __forceinline__ R round_sr(R v, uint32_t h, int i) { return decode(encode_sr(v, h, i)); }
+    __device__ static __forceinline__ R round_sr(R v, uint32_t h, int i, bool hi) { return decode(encode_sr(v, h, i, hi)); }
+    static constexpr int SCALE_LOG2 = 0;
+    __device__ static __forceinline__ R decode_lo(uint32_t w) { return __uint_as_float(w << 16); }
+    __device__ static __forceinline__ R decode_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+    __device__ static __forceinline__ uint32_t pack_sr(R lo, R hi, uint32_t rbits) { return cvt_rs_bf16x2(hi, lo, rbits); }
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -191,78 +229,235 @@ __device__ __forceinline__ double v_rcp(double a) { return __drcp_rn(a); }
 //   f*_i = f_i - w+ (f+ - feq+) - w- (f- - feq-) + S+ + S-
 // (f+- = (f_i +- f_o)/2, feq+ = w (drho + rho (4.5 cu^2 - 1.5 u.u)),
 //  feq- = 3 w rho cu, S+ = w (1 - w+/2)(9 cu cF - 3 u.F), S- = 3 w (1 - w-/2) cF)
-// is evaluated in factored form
-//   f*_i = a f_i + b f_o + E + O,   f*_o = a f_o + b f_i + E - O
-//   a = 1 - (w+ + w-)/2,  b = (w- - w+)/2
-//   E = w (A + cu (B cu + C cF)),  O = w (D cu + G cF)
-//   A = w+ (drho - 1.5 rho u.u) - 3 (1 - w+/2) u.F,  B = 4.5 w+ rho,  C = 9 (1 - w+/2)
-//   D = 3 w- rho,  G = 3 (1 - w-/2)
-// so each pair costs ~15 operations; the node-level scalars are shared. BGK
-// is w- = w+ (b = 0). The rest population: f*_0 = (1 - w+) f_0 + w_0 A.
-// u = (j + F/2) / rho uses one reciprocal per node.
-template <class L, class V>
-__device__ __forceinline__ void collide(V (&f)[L::Q], V wp, V wm,
-                                        V Fx, V Fy, V Fz)
+// is evaluated on the pair sums s = f_i + f_o and differences d = f_i - f_o,
+// which also give the moments (drho = f_0 + sum s, j = sum c_i d):
+//   P = hp s + E,  Qd = hm d + O,  f*_i = P + Qd,  f*_o = P - Qd
+//   hp = (1 - w+)/2,  hm = (1 - w-)/2
+//   E = (w A) + cu ((w B) cu + kC_i),  O = (w D) cu + kG_i
+//   A = w+ (drho - 1.5 rho u.u) - 3 (1 - w+/2) u.F,  B = 4.5 w+ rho,  D = 3 w- rho
+//   kC_i = (w 9 (1 - w+/2)) cF,  kG_i = (w 3 (1 - w-/2)) cF
+// kC and kG depend on the force only: for a uniform force they are computed
+// once per launch (relax_constants) and read as kernel parameters; w A, w B
+// and w D once per weight. About 8 operations per pair; BGK is w- = w+. The
+// rest population: f*_0 = (1 - w+) f_0 + w_0 A. One reciprocal per node.
+// Every operation rounds explicitly (host and device alike), so all kernels,
+// and constants computed on the host or per node, give the same bits.
+//
+// SCALE_LOG2 = k runs the update on populations multiplied by 2^k (float16
+// storage keeps f~ 2^14 in its format): the moments are scaled back once and
+// the weights and force terms carry 2^k. Scaling by a power of two is exact,
+// so the result is 2^k times the unscaled one, bit for bit.
+__host__ __device__ __forceinline__ float r_add(float a, float b)
 {
-    const V zero = V(0);
-    V drho = f[0], jx = zero, jy = zero, jz = zero;
-#pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        drho = v_add(drho, f[i]);
-        if (L::cx(i) > 0) jx = v_add(jx, f[i]);
-        if (L::cx(i) < 0) jx = v_sub(jx, f[i]);
-        if (L::cy(i) > 0) jy = v_add(jy, f[i]);
-        if (L::cy(i) < 0) jy = v_sub(jy, f[i]);
-        if (L::cz(i) > 0) jz = v_add(jz, f[i]);
-        if (L::cz(i) < 0) jz = v_sub(jz, f[i]);
+#ifdef __CUDA_ARCH__
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+__host__ __device__ __forceinline__ float r_sub(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+__host__ __device__ __forceinline__ float r_mul(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ double r_add(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+__host__ __device__ __forceinline__ double r_sub(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+__host__ __device__ __forceinline__ double r_mul(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+
+constexpr int QMAX = 19;
+
+// Node-independent collision constants of one launch (see above).
+template <class R>
+struct Relax {
+    R wp, one_m_wp, hp, hm, b45, d3, a3m;  // w+, 1 - w+, (1-w+)/2, (1-w-)/2, 4.5 w+, 3 w-, -3 (1 - w+/2)
+    R c9, g3;                              // 9 (1 - w+/2), 3 (1 - w-/2)
+    R kc[QMAX], kg[QMAX];                  // kC_i, kG_i of the uniform force
+    R kcs[QMAX], kgs[QMAX];                // the same times 2^14 (float16 storage)
+};
+
+// c_i . F as a sum of +-components in x, y, z order (0 - F for a negative
+// leading component, so a zero force gives +0 everywhere).
+template <class L, class R>
+__host__ __device__ __forceinline__ R guo_cf(int i, R Fx, R Fy, R Fz)
+{
+    R cF = R(0);
+    bool first = true;
+    if (L::cx(i) != 0) {
+        cF = L::cx(i) > 0 ? Fx : r_sub(R(0), Fx);
+        first = false;
     }
-    const V half = V(0.5);
-    const V rho = v_add(V(1), drho);
-    const V inv = v_rcp(rho);
-    const V ux = v_mul(v_fma(half, Fx, jx), inv);
-    const V uy = v_mul(v_fma(half, Fy, jy), inv);
-    const V uz = L::D == 3 ? v_mul(v_fma(half, Fz, jz), inv) : zero;
-    V usq = v_mul(ux, ux);
-    usq = v_fma(uy, uy, usq);
-    if (L::D == 3) usq = v_fma(uz, uz, usq);
-    V uF = v_mul(ux, Fx);
-    uF = v_fma(uy, Fy, uF);
-    if (L::D == 3) uF = v_fma(uz, Fz, uF);
-    // Node-independent constants, also with explicit rounding: a contracted
-    // 1 - w/2 in one kernel and an uncontracted one in another would differ.
-    const V ap = v_sub(V(1), v_mul(V(0.5), wp)), am = v_sub(V(1), v_mul(V(0.5), wm));
-    // A = w+ (drho - 1.5 rho usq) - 3 ap uF
-    const V A = v_fma(v_mul(V(-3), ap), uF, v_mul(wp, v_fma(v_mul(V(-1.5), rho), usq, drho)));
-    const V B = v_mul(v_mul(V(4.5), wp), rho);
-    const V C = v_mul(V(9), ap);
-    const V Dm = v_mul(v_mul(V(3), wm), rho);
-    const V G = v_mul(V(3), am);
-    const V ca = v_sub(V(1), v_mul(V(0.5), v_add(wp, wm)));
-    const V cb = v_mul(V(0.5), v_sub(wm, wp));
-    f[0] = v_fma(v_sub(V(1), wp), f[0], v_mul(V(L::w(0)), A));
+    if (L::cy(i) != 0) {
+        if (first) cF = L::cy(i) > 0 ? Fy : r_sub(R(0), Fy);
+        else cF = L::cy(i) > 0 ? r_add(cF, Fy) : r_sub(cF, Fy);
+        first = false;
+    }
+    if (L::D == 3 && L::cz(i) != 0) {
+        if (first) cF = L::cz(i) > 0 ? Fz : r_sub(R(0), Fz);
+        else cF = L::cz(i) > 0 ? r_add(cF, Fz) : r_sub(cF, Fz);
+    }
+    return cF;
+}
+
+template <class L, class R>
+__host__ __device__ inline void relax_scalars(Relax<R>& r, double wp_d, double wm_d)
+{
+    const R wp = R(wp_d), wm = R(wm_d);
+    r.wp = wp;
+    r.one_m_wp = r_sub(R(1), wp);
+    r.hp = r_mul(R(0.5), r.one_m_wp);
+    r.hm = r_mul(R(0.5), r_sub(R(1), wm));
+    r.b45 = r_mul(R(4.5), wp);
+    r.d3 = r_mul(R(3), wm);
+    const R ap = r_sub(R(1), r_mul(R(0.5), wp)), am = r_sub(R(1), r_mul(R(0.5), wm));
+    r.a3m = r_mul(R(-3), ap);
+    r.c9 = r_mul(R(9), ap);
+    r.g3 = r_mul(R(3), am);
+}
+
+template <class L, class R>
+__host__ __device__ inline void relax_constants(Relax<R>& r, double wp, double wm, double fx, double fy, double fz)
+{
+    relax_scalars<L, R>(r, wp, wm);
+    for (int i = 0; i < QMAX; ++i) {
+        R kc = R(0), kg = R(0);
+        if (i < L::Q) {
+            const R cF = guo_cf<L, R>(i, R(fx), R(fy), R(fz));
+            kc = r_mul(r_mul(R(L::w(i)), r.c9), cF);
+            kg = r_mul(r_mul(R(L::w(i)), r.g3), cF);
+        }
+        r.kc[i] = kc;
+        r.kg[i] = kg;
+        r.kcs[i] = r_mul(kc, R(16384));
+        r.kgs[i] = r_mul(kg, R(16384));
+    }
+}
+
+// Force terms of the collision: from the launch constants (uniform force) ...
+template <class R, int SCALE_LOG2>
+struct UniformGuo {
+    const Relax<R>& r;
+    __device__ __forceinline__ R kc(int i) const { return SCALE_LOG2 ? r.kcs[i] : r.kc[i]; }
+    __device__ __forceinline__ R kg(int i) const { return SCALE_LOG2 ? r.kgs[i] : r.kg[i]; }
+};
+// ... or computed for this node's force (per-node force fields)
+template <class L, class R, int SCALE_LOG2>
+struct NodeGuo {
+    const Relax<R>& r;
+    R Fx, Fy, Fz;
+    __device__ __forceinline__ R k(int i, R coef) const
+    {
+        const R v = r_mul(r_mul(R(L::w(i)), coef), guo_cf<L, R>(i, Fx, Fy, Fz));
+        return SCALE_LOG2 ? r_mul(v, R(1 << SCALE_LOG2)) : v;
+    }
+    __device__ __forceinline__ R kc(int i) const { return k(i, r.c9); }
+    __device__ __forceinline__ R kg(int i) const { return k(i, r.g3); }
+};
+
+template <class L, class R, int SCALE_LOG2, class Guo>
+__device__ __forceinline__ void collide(R (&f)[L::Q], const Relax<R>& c, R Fx, R Fy, R Fz, const Guo& guo)
+{
+    constexpr double SC = (double)(1 << SCALE_LOG2);
+    R s[L::Q], d[L::Q];
+    R drho = f[0];
+    R jx = R(0), jy = R(0), jz = R(0);
+    bool fx = true, fy = true, fz = true;
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
         const int o = L::opp(i);
         if (o < i) continue;
-        const V wi = V(L::w(i));
-        // cu, cF: sums of +-components (exact sign flips, no multiplies)
-        V cu = zero, cF = zero;
-        bool first = true;
-        if (L::cx(i) != 0) { cu = L::cx(i) > 0 ? ux : v_sub(zero, ux); cF = L::cx(i) > 0 ? Fx : v_sub(zero, Fx); first = false; }
-        if (L::cy(i) != 0) {
-            if (first) { cu = L::cy(i) > 0 ? uy : v_sub(zero, uy); cF = L::cy(i) > 0 ? Fy : v_sub(zero, Fy); first = false; }
-            else { cu = L::cy(i) > 0 ? v_add(cu, uy) : v_sub(cu, uy); cF = L::cy(i) > 0 ? v_add(cF, Fy) : v_sub(cF, Fy); }
-        }
-        if (L::cz(i) != 0) {
-            if (first) { cu = L::cz(i) > 0 ? uz : v_sub(zero, uz); cF = L::cz(i) > 0 ? Fz : v_sub(zero, Fz); }
-            else { cu = L::cz(i) > 0 ? v_add(cu, uz) : v_sub(cu, uz); cF = L::cz(i) > 0 ? v_add(cF, Fz) : v_sub(cF, Fz); }
-        }
-        const V E = v_mul(wi, v_fma(cu, v_fma(B, cu, v_mul(C, cF)), A));
-        const V O = v_mul(wi, v_fma(Dm, cu, v_mul(G, cF)));
-        const V fi = f[i], fo = f[o];
-        f[i] = v_fma(ca, fi, v_fma(cb, fo, v_add(E, O)));
-        f[o] = v_fma(ca, fo, v_fma(cb, fi, v_sub(E, O)));
+        s[i] = v_add(f[i], f[o]);
+        d[i] = v_sub(f[i], f[o]);
+        drho = v_add(drho, s[i]);
+        // j = sum c_i d over pairs (c_o = -c_i)
+        if (L::cx(i) != 0) { jx = fx ? (L::cx(i) > 0 ? d[i] : -d[i]) : (L::cx(i) > 0 ? v_add(jx, d[i]) : v_sub(jx, d[i])); fx = false; }
+        if (L::cy(i) != 0) { jy = fy ? (L::cy(i) > 0 ? d[i] : -d[i]) : (L::cy(i) > 0 ? v_add(jy, d[i]) : v_sub(jy, d[i])); fy = false; }
+        if (L::D == 3 && L::cz(i) != 0) { jz = fz ? (L::cz(i) > 0 ? d[i] : -d[i]) : (L::cz(i) > 0 ? v_add(jz, d[i]) : v_sub(jz, d[i])); fz = false; }
     }
+    if (SCALE_LOG2) {
+        const R inv_sc = R(1.0 / SC);
+        drho = v_mul(drho, inv_sc);
+        jx = v_mul(jx, inv_sc);
+        jy = v_mul(jy, inv_sc);
+        if (L::D == 3) jz = v_mul(jz, inv_sc);
+    }
+    const R half = R(0.5);
+    const R rho = v_add(R(1), drho);
+    const R inv = v_rcp(rho);
+    const R ux = v_mul(v_fma(half, Fx, jx), inv);
+    const R uy = v_mul(v_fma(half, Fy, jy), inv);
+    const R uz = L::D == 3 ? v_mul(v_fma(half, Fz, jz), inv) : R(0);
+    R usq = v_mul(ux, ux);
+    usq = v_fma(uy, uy, usq);
+    if (L::D == 3) usq = v_fma(uz, uz, usq);
+    R uF = v_mul(ux, Fx);
+    uF = v_fma(uy, Fy, uF);
+    if (L::D == 3) uF = v_fma(uz, Fz, uF);
+    // A = w+ (drho - 1.5 rho usq) - 3 (1 - w+/2) uF
+    const R A = v_fma(c.a3m, uF, v_mul(c.wp, v_fma(v_mul(R(-1.5), rho), usq, drho)));
+    const R B = v_mul(c.b45, rho);
+    const R Dm = v_mul(c.d3, rho);
+    f[0] = v_fma(c.one_m_wp, f[0], v_mul(R(L::w(0) * SC), A));
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        const int o = L::opp(i);
+        if (o < i) continue;
+        const R wi = R(L::w(i) * SC);
+        R cu = R(0);
+        bool first = true;
+        if (L::cx(i) != 0) { cu = L::cx(i) > 0 ? ux : -ux; first = false; }
+        if (L::cy(i) != 0) { cu = first ? (L::cy(i) > 0 ? uy : -uy) : (L::cy(i) > 0 ? v_add(cu, uy) : v_sub(cu, uy)); first = false; }
+        if (L::D == 3 && L::cz(i) != 0) cu = first ? (L::cz(i) > 0 ? uz : -uz) : (L::cz(i) > 0 ? v_add(cu, uz) : v_sub(cu, uz));
+        const R E = v_fma(cu, v_fma(v_mul(wi, B), cu, guo.kc(i)), v_mul(wi, A));
+        const R O = v_fma(v_mul(wi, Dm), cu, guo.kg(i));
+        const R P = v_fma(c.hp, s[i], E);
+        const R Qd = v_fma(c.hm, d[i], O);
+        f[i] = v_add(P, Qd);
+        f[o] = v_sub(P, Qd);
+    }
+}
+
+// Collision of one node whose force is (Fx, Fy, Fz): the launch's force
+// terms when that is the uniform force and they were precomputed, else per
+// node.
+template <class L, class R, int SCALE_LOG2 = 0>
+__device__ __forceinline__ void collide_node(R (&f)[L::Q], const Relax<R>& c, bool uniform, R Fx, R Fy, R Fz)
+{
+    if (uniform)
+        collide<L, R, SCALE_LOG2>(f, c, Fx, Fy, Fz, UniformGuo<R, SCALE_LOG2>{c});
+    else
+        collide<L, R, SCALE_LOG2>(f, c, Fx, Fy, Fz, NodeGuo<L, R, SCALE_LOG2>{c, Fx, Fy, Fz});
 }
 
 // Moving-wall (Ladd) term 6 w_i (c_i . u_w) with u_w read at solid node s,
@@ -299,6 +494,16 @@ struct StepArgs {
     uint32_t* seed;
     int parity;
     lbm_special_t sp;
+    bool guo_const;    // rf/rd hold kC, kG of the uniform force (else computed per node)
+    Relax<float> rf;   // collision constants (float arithmetic)
+    Relax<double> rd;  // the same for float64 storage
+    template <class R> __device__ __forceinline__ const Relax<R>& relax() const
+    {
+        if constexpr (sizeof(R) == 8)
+            return rd;
+        else
+            return rf;
+    }
 };
 
 // The bulk (or fused) launch of a step advances the step counter: one thread

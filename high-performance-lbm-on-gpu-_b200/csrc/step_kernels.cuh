@@ -65,7 +65,7 @@ struct StepKernel {
     // the same for all threads (-c_i . strides), so the compiler keeps them in
     // uniform registers and each access is [thread pointer + uniform offset].
     // All Q loads are independent and issued back to back.
-    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd, int64_t natural)
+    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd, int64_t pair, bool hi)
     {
         const int64_t qs = a.qstride;
         const int64_t py = a.pitch;
@@ -89,18 +89,18 @@ struct StepKernel {
             Fy += ff[qs + nd];
             if (L::D == 3) Fz += ff[2 * qs + nd];
         }
-        collide<L, R>(f, R(a.wp), R(a.wm), Fx, Fy, Fz);
-        const uint32_t h = S::STOCHASTIC ? sr_node_hash(natural, a.seed[a.parity]) : 0u;
+        collide_node<L, R>(f, a.template relax<R>(), a.guo_const && a.force_field == nullptr, Fx, Fy, Fz);
+        const uint32_t h = S::STOCHASTIC ? sr_pair_hash(pair, a.seed[a.parity]) : 0u;
         T* fd = static_cast<T*>(a.f_dst) + nd;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const int64_t shift = L::cx(i) + L::cy(i) * py + L::cz(i) * pz;
             if (VAR == LBM_PULL)
-                S::store_sr(fd + i * qs, f[i], h, i);
+                S::store_sr(fd + i * qs, f[i], h, i, hi);
             else if (VAR == LBM_AA_EVEN)
-                S::store_sr(fd + L::opp(i) * qs, f[i], h, i);
+                S::store_sr(fd + L::opp(i) * qs, f[i], h, i, hi);
             else
-                S::store_sr(fd + (i * qs + shift), f[i], h, i);
+                S::store_sr(fd + (i * qs + shift), f[i], h, i, hi);
         }
     }
 
@@ -171,9 +171,11 @@ struct StepKernel {
             Fy += ff[qs + nd];
             if (L::D == 3) Fz += ff[2 * qs + nd];
         }
+        bool uniform = a.guo_const && a.force_field == nullptr;
         if (SPECIAL) {
             const int fs = a.sp.force_slot[s];
             if (fs >= 0) {
+                uniform = false;
                 const R* lf = static_cast<const R*>(a.sp.local_force);
                 const int64_t n = a.sp.n_local;
                 Fx += lf[fs];
@@ -181,17 +183,18 @@ struct StepKernel {
                 if (L::D == 3) Fz += lf[2 * n + fs];
             }
         }
-        collide<L, R>(f, R(a.wp), R(a.wm), Fx, Fy, Fz);
-        const uint32_t h = S::STOCHASTIC ? sr_node_hash(((int64_t)z * a.ny + y) * a.nx + x, a.seed[a.parity]) : 0u;
+        collide_node<L, R>(f, a.template relax<R>(), uniform, Fx, Fy, Fz);
+        const uint32_t h = S::STOCHASTIC ? sr_pair_hash(sr_pair(a.nx, a.ny, x, y, z), a.seed[a.parity]) : 0u;
+        const bool hi = x & 1;
 
-        // ---- store (16-bit formats: stochastic rounding, see sr_node_hash)
+        // ---- store (16-bit formats: stochastic rounding, see sr_pair_hash)
         T* fd = static_cast<T*>(a.f_dst);
         if (VAR == LBM_PULL) {
 #pragma unroll
-            for (int i = 0; i < Q; ++i) S::store_sr(fd + i * qs + nd, f[i], h, i);
+            for (int i = 0; i < Q; ++i) S::store_sr(fd + i * qs + nd, f[i], h, i, hi);
         } else if (VAR == LBM_AA_EVEN) {
 #pragma unroll
-            for (int i = 0; i < Q; ++i) S::store_sr(fd + L::opp(i) * qs + nd, f[i], h, i);
+            for (int i = 0; i < Q; ++i) S::store_sr(fd + L::opp(i) * qs + nd, f[i], h, i, hi);
         } else {
 #pragma unroll
             for (int i = 0; i < Q; ++i) {
@@ -200,9 +203,9 @@ struct StepKernel {
                 const int dz = L::cz(i) > 0 ? zp : (L::cz(i) < 0 ? zm : z);
                 const int64_t dst = ((int64_t)dz * a.ny + dy) * a.pitch + dx;
                 if (i != 0 && ((bb >> L::opp(i)) & 1u)) {
-                    S::store_sr(fd + L::opp(i) * qs + nd, v_add(f[i], wall_term<L, R>(L::opp(i), wall, dst, qs)), h, i);
+                    S::store_sr(fd + L::opp(i) * qs + nd, v_add(f[i], wall_term<L, R>(L::opp(i), wall, dst, qs)), h, i, hi);
                 } else {
-                    S::store_sr(fd + i * qs + dst, f[i], h, i);
+                    S::store_sr(fd + i * qs + dst, f[i], h, i, hi);
                 }
             }
         }
@@ -221,7 +224,7 @@ struct StepKernel {
 #pragma unroll
                     for (int j = 1; j < Q; ++j)
                         if (j == k) v = f[j];
-                    out[e++] = S::round_sr(v, h, k);
+                    out[e++] = S::round_sr(v, h, k, hi);
                 }
             }
         }
@@ -240,7 +243,7 @@ __device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z
     using K = StepKernel<L, ST, VAR>;
     const uint8_t k = in ? a.kind[nd] : KIND_SOLID;
     if (__all_sync(0xffffffffu, !in || k == KIND_FLUID)) {
-        if (in) K::interior(a, nd, ((int64_t)z * a.ny + y) * a.nx + x);
+        if (in) K::interior(a, nd, sr_pair(a.nx, a.ny, x, y, z), x & 1);
     } else if (!(k & (KIND_SOLID | KIND_SPECIAL))) {
         K::template node<false>(a, x, y, z, nd, a.nbr[nd], -1);
     }
@@ -255,6 +258,108 @@ __device__ __forceinline__ void bulk_tile(const StepArgs& a, int z)
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     bulk_node<L, ST, VAR>(a, x, y, z, ((int64_t)z * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny);
 }
+
+// ---------------------------------------------------------------- vector pull
+// Two-lattice pull for 16-bit storage with the two nodes of a pair (x even,
+// x + 1) per thread: one 4-byte load and one 4-byte store per direction move
+// both populations, the two collisions are independent (instruction-level
+// parallelism), and one cvt.rs converts both results with stochastic
+// rounding (see sr_pair_hash). A warp covers 64 nodes of one row.
+//   * Links along y and z read the aligned pair of the shifted row.
+//   * Links along x need the pair shifted by one node: it is rebuilt from the
+//     thread's own word and one word of the neighbouring lane (warp shuffle);
+//     lanes 0 and 31 load the one node beyond the warp's range themselves,
+//     with x wrapped on the periodic faces.
+// The vector path runs when every node of the warp's range is interior or on
+// a periodic x face (kinds 0 and EDGE, rows off the y and z faces), the
+// range lies inside [0, nx) and the force is uniform (the launch picks the
+// one-node kernel for per-node force fields); any other warp updates its
+// nodes one at a time (bulk_node), lane l taking nodes x_base + 32 k + l so
+// that accesses stay coalesced. float16 runs the collision on populations
+// times 2^14, which is exact. Per node the arithmetic and the rounding are
+// those of the one-node paths: the bits do not depend on the path.
+template <class L, int ST>
+struct VecPull {
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    static constexpr int Q = L::Q;
+    static constexpr int V = 2;
+    static_assert(sizeof(T) == 2, "two 16-bit populations per word");
+
+    __device__ static __forceinline__ void run(const StepArgs& a, int x_base, int y, int z)
+    {
+        constexpr unsigned FULL = 0xffffffffu;
+        const int lane = threadIdx.x & 31;
+        const int64_t qs = a.qstride;
+        const int64_t py = a.pitch;
+        const int64_t pz = (int64_t)a.pitch * a.ny;
+        const int64_t row = (int64_t)z * pz + (int64_t)y * py;
+        const int x0 = x_base + V * lane;
+        const int64_t nd0 = row + x0;
+        const bool in_row = y < a.ny;
+        bool fast = in_row && x_base + 32 * V <= a.nx && y > 0 && y < a.ny - 1 &&
+                    (L::D == 2 || (z > 0 && z < a.nz - 1));
+        if (fast) fast = (*reinterpret_cast<const unsigned short*>(a.kind + nd0) & ~0x0808u) == 0u;
+        if (!__all_sync(FULL, fast)) {
+            for (int j = 0; j < V; ++j) {
+                const int x = x_base + 32 * j + lane;
+                bulk_node<L, ST, LBM_PULL>(a, x, y, z, row + x, in_row && x < a.nx);
+            }
+            return;
+        }
+        // periodic x: the nodes just outside the warp's range
+        const int x_lo = x_base == 0 ? a.nx - 1 : x_base - 1;
+        const int x_hi = x_base + 32 * V == a.nx ? 0 : x_base + 32 * V;
+        const T* fs = static_cast<const T*>(a.f_src);
+        R fa[Q], fb[Q];  // the even and the odd node
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int64_t shifted_row = row - (L::cy(i) * py + L::cz(i) * pz) + i * qs;
+            const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(fs + shifted_row + x0));
+            uint32_t s = w;
+            if (L::cx(i) > 0) {  // sources x - 1: (own first, last of lane - 1)
+                uint32_t pw = __shfl_up_sync(FULL, w, 1);
+                if (lane == 0) pw = (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(fs + shifted_row + x_lo)) << 16;
+                s = __byte_perm(pw, w, 0x5432);
+            } else if (L::cx(i) < 0) {  // sources x + 1: (first of lane + 1, own last)
+                uint32_t nw = __shfl_down_sync(FULL, w, 1);
+                if (lane == 31) nw = __ldg(reinterpret_cast<const unsigned short*>(fs + shifted_row + x_hi));
+                s = __byte_perm(w, nw, 0x5432);
+            }
+            fa[i] = S::decode_lo(s);
+            fb[i] = S::decode_hi(s);
+        }
+        const Relax<R>& rc = a.template relax<R>();
+        const R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
+        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        const uint32_t h = sr_pair_hash(sr_pair(a.nx, a.ny, x0, y, z), a.seed[a.parity]);
+        T* fd = static_cast<T*>(a.f_dst) + nd0;
+#pragma unroll
+        for (int i = 0; i < Q; ++i)
+            *reinterpret_cast<uint32_t*>(fd + i * qs) = S::pack_sr(fa[i], fb[i], sr_word(h, i));
+    }
+};
+
+// Vector bulk launch: grid (ceil(nx / (2 tile_x)), ceil(ny / tile_y), nz).
+template <class L, int ST>
+__global__ void __launch_bounds__(256) lbm_bulk_vec_kernel(const StepArgs a)
+{
+    advance_seed(a);
+    const int warp_x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    VecPull<L, ST>::run(a, warp_x * 64, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
+}
+
+// Storage formats with the pair and TMA kernels (float32 and float64 keep
+// the one-node kernel: it is faster there).
+template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_BF16; }
+
+}  // namespace lbm
+
+#include "tma_pull.cuh"
+
+namespace lbm {
 
 template <class L, int ST, int VAR>
 __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
@@ -309,6 +414,17 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
         lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY><<<(unsigned)blocks, 256, 0, stream>>>(a);
     } else if (mode == LBM_LAUNCH_BULK) {
         if (a.nz > 65535) return LBM_ERR_INVALID;
+        if constexpr (VAR == LBM_PULL && has_vec<ST>()) {
+            int status = LBM_OK;
+            if (launch_tma_pull<L, ST>(a, stream, &status)) return status;
+            // pairs need every row and direction plane to start on an even
+            // node, and the launch's uniform-force constants
+            if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
+                const unsigned gxv = (unsigned)((a.nx + 2 * tile_x - 1) / (2 * tile_x));
+                lbm_bulk_vec_kernel<L, ST><<<dim3(gxv, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+                return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+            }
+        }
         lbm_bulk_kernel<L, ST, VAR><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
     } else {
         const int64_t per_plane = (int64_t)gx * gy * threads;

@@ -202,7 +202,9 @@ class CudaSolver(Solver):
         nx = shape[-1]
         ny = shape[-2]
         nz = shape[0] if d == 3 else 1
-        self.pitch = int(pitch) if pitch is not None else nx
+        # 16-bit rows padded to a multiple of 16 nodes: the pair kernel and the
+        # TMA tile loads (populations and kind bytes) need 16-byte row strides
+        self.pitch = int(pitch) if pitch is not None else (-(-nx // 16) * 16 if params.dtype in ("float16", "bfloat16") else nx)
         if self.pitch < nx:
             raise ValueError(f"pitch must be >= nx={nx}; got {self.pitch}")
         self.qstride = self.pitch * ny * nz
@@ -226,9 +228,9 @@ class CudaSolver(Solver):
         if force_field is not None:
             self._force_field = self._upload_field(np.asarray(force_field, dtype=np.float64).reshape(d, *shape))
         self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field), None)
-        # step counter (two slots) of the stochastic rounding of 16-bit storage;
-        # reset whenever the populations are set
-        self._seed = torch.zeros(2, dtype=torch.int32, device=self.device)
+        # step counter (slots 0, 1) of the stochastic rounding of 16-bit storage,
+        # reset whenever the populations are set; slot 2: kernel status word
+        self._seed = torch.zeros(4, dtype=torch.int32, device=self.device)
         self.physics.round_seed = N.ptr(self._seed)
 
         # ---- immersed boundary and link rules -> special nodes
@@ -462,7 +464,7 @@ class CudaSolver(Solver):
         self._after_state_change()
 
     def _after_state_change(self):
-        self._seed.zero_()
+        self._seed[:2].zero_()
         s = self._special
         if self.variant == "aa" and s.n_export:
             self._export_cur = s.tensors["export_a"]
@@ -595,6 +597,8 @@ class CudaSolver(Solver):
         self._native("lbm_health_reset", N.ptr(self._health), self._stream())
         self._native("lbm_health", N.C.byref(self.grid), N.ptr(self._kind), N.ptr(self._f), N.ptr(self._health), self._stream())
         first, nonfinite = (int(v) for v in self._health.cpu().tolist())
+        if int(self._seed[2].item()) != 0:
+            raise N.NativeError("a step kernel gave up waiting for its staged tiles (TMA loads did not arrive)")
         if first == 2**63 - 1:
             return
         location = _natural_index(first, self.shape, self.pitch)

@@ -43,7 +43,7 @@ def quantize(f: np.ndarray, dtype: str) -> np.ndarray:
     return f
 
 
-SR_GOLDEN = 0x9E3779B9
+SR_MULT = 0x9E3779B9
 
 
 def lowbias32(x):
@@ -57,33 +57,59 @@ def lowbias32(x):
     return x
 
 
+def sr_keys(q: int) -> np.ndarray:
+    """Per-direction keys K_i = lowbias32(i + 1)."""
+    return lowbias32(np.arange(1, q + 1, dtype=np.uint32))
+
+
+def _float16_stochastic(v: np.ndarray, r: np.ndarray) -> np.ndarray:
+    """float32 -> float16 as cvt.rs rounds: |v| + r 2^-13 ulp(|v|), truncated; >= 65536 -> inf."""
+    a = np.abs(v.astype(np.float64))
+    _, ex = np.frexp(a)
+    ulp = np.ldexp(1.0, np.maximum(ex - 1, -14) - 10)
+    with np.errstate(invalid="ignore"):
+        y = a + r.astype(np.float64) * ulp / 8192.0
+        q = np.floor(y / ulp) * ulp
+    q = np.where(q >= 65536.0, np.inf, q)
+    return np.copysign(q, v).astype(np.float16)
+
+
 def stochastic_round(f: np.ndarray, dtype: str, step: int) -> np.ndarray:
     """Stochastic rounding of post-collision populations to 16-bit storage, as the step kernels store them.
 
-    f has shape (q, *shape) in natural order. For node n (flat index) at
-    step t: h = lowbias32(n ^ lowbias32(t)); direction i adds the top 13
-    (float16, after the 2^14 scale) or 16 (bfloat16) bits of h * (golden *
-    (2i + 1)) mod 2^32 below the kept mantissa bits, then truncates.
-    float32/float64 storage is returned unchanged.
+    f has shape (q, *shape) in natural order (x last). Nodes pair up along x
+    (x even with x + 1): pair = row * ceil(nx / 2) + x // 2, h =
+    lowbias32(pair ^ lowbias32(step)) and direction i draws the 32-bit word
+    (h ^ K_i) * 0x9E3779B9; the even node takes bits 0-12 (float16, after the
+    2^14 scale; 0-15 for bfloat16) as r, the odd node bits 16-28 (16-31).
+    float16: |v| + r 2^-13 ulp(|v|) truncated toward zero, magnitudes that
+    reach 65536 infinite; bfloat16: r added to the float32 bit pattern, then
+    truncated. float32/float64 storage is returned unchanged.
     """
     if dtype not in ("float16", "bfloat16"):
         return f
     q = f.shape[0]
-    flat = f.reshape(q, -1)
-    node = np.arange(flat.shape[1], dtype=np.uint64).astype(np.uint32)
-    h = lowbias32(node ^ lowbias32(np.uint32(step & 0xFFFFFFFF)))
+    nx = f.shape[-1]
+    rows = int(np.prod(f.shape[1:-1], dtype=np.int64))
+    flat = f.reshape(q, rows, nx)
+    x = np.arange(nx, dtype=np.int64)
+    pair = (np.arange(rows, dtype=np.int64)[:, None] * ((nx + 1) // 2) + (x // 2)[None, :]).astype(np.uint32)
+    odd = np.broadcast_to((x & 1).astype(bool)[None, :], (rows, nx))
+    h = lowbias32(pair ^ lowbias32(np.uint32(step & 0xFFFFFFFF)))
+    keys = sr_keys(q)
     out = np.empty(flat.shape, dtype=np.float32)
     with np.errstate(over="ignore"):
         for i in range(q):
-            mult = np.uint32((SR_GOLDEN * (2 * i + 1)) & 0xFFFFFFFF)
-            x = flat[i].astype(np.float32)
+            word = (h ^ keys[i]) * np.uint32(SR_MULT)
+            xi = flat[i].astype(np.float32)
             if dtype == "float16":
-                x = x * np.float32(FP16_SCALE)
-                bits = (x.view(np.uint32) + ((h * mult) >> np.uint32(19))) & np.uint32(0xFFFFE000)
-                out[i] = bits.view(np.float32).astype(np.float16).astype(np.float32) * np.float32(1.0 / FP16_SCALE)
+                r = np.where(odd, (word >> np.uint32(16)) & np.uint32(0x1FFF), word & np.uint32(0x1FFF))
+                scaled = xi * np.float32(FP16_SCALE)
+                out[i] = _float16_stochastic(scaled, r).astype(np.float32) * np.float32(1.0 / FP16_SCALE)
             else:
-                bits = (x.view(np.uint32) + ((h * mult) >> np.uint32(16))) & np.uint32(0xFFFF0000)
-                out[i] = bits.view(np.float32)
+                r = np.where(odd, word >> np.uint32(16), word & np.uint32(0xFFFF))
+                bits = (xi.view(np.uint32).astype(np.uint64) + r.astype(np.uint64)) >> np.uint64(16) << np.uint64(16)
+                out[i] = bits.astype(np.uint32).view(np.float32)
     return out.reshape(f.shape)
 
 

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from oracle import lowbias32, stochastic_round
-from oracle.lbm_oracle import FP16_SCALE, SR_GOLDEN
+from oracle.lbm_oracle import FP16_SCALE, SR_MULT, sr_keys
 
 ROOT = Path(__file__).resolve().parent.parent
 
@@ -62,13 +62,14 @@ def test_wider_formats_are_not_rounded():
 
 @pytest.mark.skipif(shutil.which("nvcc") is None, reason="needs nvcc")
 def test_device_hash_matches_the_oracle(tmp_path):
-    """lowbias32 and the direction multipliers of lbm_common.cuh, run on the host, equal the NumPy ones."""
+    """lowbias32, the direction keys and the multiplier of lbm_common.cuh, run on the host, equal the NumPy ones."""
     src = tmp_path / "hash.cu"
     src.write_text(
         '#include "lbm_common.cuh"\n#include <cstdio>\n'
         "int main() { const unsigned xs[] = {0u, 1u, 2u, 12345u, 4000000000u, 0xffffffffu};\n"
         '  for (unsigned x : xs) printf("%u\\n", lbm::lowbias32(x));\n'
-        '  for (int i = 0; i < 19; ++i) printf("%u\\n", lbm::sr_mult(i));\n  return 0; }\n'
+        '  for (int i = 0; i < 19; ++i) printf("%u\\n", lbm::sr_key(i));\n'
+        '  printf("%u\\n", lbm::SR_MULT);\n  return 0; }\n'
     )
     exe = tmp_path / "hash"
     csrc = ROOT / "high-performance-lbm-on-gpu-_b200" / "csrc"
@@ -77,4 +78,14 @@ def test_device_hash_matches_the_oracle(tmp_path):
     vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     xs = np.array([0, 1, 2, 12345, 4000000000, 0xFFFFFFFF], dtype=np.uint64).astype(np.uint32)
     assert vals[:6] == [int(v) for v in lowbias32(xs)]
-    assert vals[6:] == [(SR_GOLDEN * (2 * i + 1)) & 0xFFFFFFFF for i in range(19)]
+    assert vals[6:25] == [int(v) for v in sr_keys(19)]
+    assert vals[25] == SR_MULT
+
+
+def test_pairs_share_a_word_but_not_their_bits():
+    """Neighbouring nodes of a pair round with different halves of the same random word."""
+    x = np.full((19, 2, 4096), 1.0 + 0.5 * 2.0**-10, dtype=np.float32) / np.float32(2.0**14)
+    out = stochastic_round(x.reshape(19, 2 * 4096), "float16", step=5).reshape(19, 2, 4096)
+    up = out > x
+    assert abs(up.mean() - 0.5) < 0.02
+    assert abs(np.mean(up[:, 0] == up[:, 1]) - 0.5) < 0.03  # even and odd nodes decide independently
