@@ -34,9 +34,14 @@
 
 namespace lbm {
 
-constexpr int TMA_ROWS = 4;
-constexpr int TMA_THREADS = 512;
-constexpr int TMA_STAGES = 4;  // tiles in flight per block: TMA_STAGES - 1 ahead of the one computed
+// Tile shape and pipeline depth, from a sweep on B200 (256^3 duct, float16):
+// 2-row tiles, 128 threads, 2 stages and 5 blocks per SM (200 KB of shared
+// memory) measured 71 GLUPS; 4-row tiles or 256-512 threads with deeper
+// pipelines and fewer blocks per SM 47-66 GLUPS.
+constexpr int TMA_ROWS = 2;
+constexpr int TMA_THREADS = 128;
+constexpr int TMA_STAGES = 2;  // tiles in flight per block: TMA_STAGES - 1 ahead of the one computed
+constexpr int TMA_BLOCKS_PER_SM = 5;
 constexpr uint32_t TMA_WAIT_LIMIT = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -134,7 +139,7 @@ __device__ __forceinline__ void bounce(const StepArgs& a, typename Storage<ST>::
 }
 
 template <class L, int ST>
-__global__ void __launch_bounds__(TMA_THREADS, 1) lbm_tma_pull_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_kernel(const __grid_constant__ CUtensorMap map,
                                                                       const __grid_constant__ CUtensorMap kmap,
                                                                       const StepArgs a, uint32_t* status)
 {
