@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="skip the batched-cavities study (aggregate MLUPS against separate launches)")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the adjoint-configuration study (forward/backward cost and finite differences)")
     ap.add_argument("--precision-steps", type=int, default=5000,
                     help="steps of the storage-precision study (0 = skip)")
     return ap.parse_args()
@@ -195,6 +199,13 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def step_kernel_name(args) -> str:
+    """The kernel that carries the duct step (one launch per step)."""
+    if args.variant == "pull" and args.storage in ("float16", "bfloat16") and args.launch == "split":
+        return f"lbm_tma_pull_kernel<D3Q19, {args.storage}>"
+    return f"lbm_bulk_kernel<D3Q19, {args.storage}, {args.variant}>"
+
+
 def profile_traffic(variant: str, storage: str):
     """DRAM bytes per launch from the committed ncu summary, if one exists for this kernel/workload."""
     path = ROOT / "profiles" / f"step_{variant}_d3q19_{storage}_duct.md"
@@ -255,6 +266,109 @@ def precision_study(lbm, torch, n: int, steps: int, variant: str):
     out["steps"] = steps
     out["u_max_f64"] = float(np.abs(ref[0]).max())
     return out
+
+
+def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: int = 100):
+    """Adjoint configuration: D3Q19 channel 128 x 64 x 64, Bouzidi sphere r = 8, Zou-He inlet U = 0.04,
+    pressure outlet, tau = 0.6, loss = drag averaged over the last `window` of `steps` steps,
+    gradients w.r.t. the inlet-speed scale U and a per-node Guo force field G ~ N(0, 1e-7^2).
+
+    float32: forward and backward (recompute + adjoint kernels) timed with CUDA events, host-driven
+    as a user calls them. float64: adjoint dL/dU and dL/dG.v against central differences (h = 1e-4
+    relative).
+    """
+    from lbm_b200.adjoint import AdjointRun, aligned_rules
+
+    lat = lbm.D3Q19
+    nx, ny, nz = 128, 64, 64
+    solid = lbm.duct_walls(nx, ny, nz)
+    body = lbm.sphere(nx / 4.0, (ny - 1) / 2.0, (nz - 1) / 2.0, 8.0)
+    solid |= lbm.voxelize(body, solid.shape)
+    inflow = np.zeros((3, nz, ny))
+    inflow[0, 1:-1, 1:-1] = 0.04
+
+    def case(dtype):
+        def make(scale):
+            s2, rules, d_rules = lbm.zou_he_inlet_derivative(lat, solid, scale * inflow)
+            links = lbm.wall_links(lat, body, s2)
+            all_rules, all_d = aligned_rules(rules, d_rules, lbm.bouzidi_rules(lat, links, s2))
+            p = lbm.SimulationParams(nx=nx, ny=ny, nz=nz, tau=0.6, collision="trt", solid=s2, dtype=dtype,
+                                     link_rules=all_rules)
+            return p, all_d
+        p, _ = make(1.0)
+        return make, lbm.wall_links(lat, body, p.solid), p
+
+    out = {"config": f"D3Q19 {nx}x{ny}x{nz} sphere r=8 (Bouzidi), Zou-He U=0.04, tau=0.6, {steps} steps, "
+                     f"drag mean over last {window}, checkpoint every {checkpoint}"}
+    make, links, p = case("float32")
+    rng = np.random.default_rng(0)
+    G = 1e-7 * rng.standard_normal((3, *p.shape)) * p.fluid
+    run = AdjointRun(make, links, steps=steps, window=window, checkpoint=checkpoint)
+    run.forward(1.0, G)  # warm-up: set-up and tables (later forwards at the same U reuse them)
+    run.backward()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    loss = run.forward(1.0, G)
+    ev[1].record()
+    dU, dG = run.backward()
+    ev[2].record()
+    ev[2].synchronize()
+    fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    out["float32"] = {"loss": loss, "dL_dU": dU, "forward_ms_per_step": round(fwd / steps, 5),
+                      "backward_ms_per_step": round(bwd / steps, 5), "backward_over_forward": round(bwd / fwd, 3)}
+    make64, links64, p64 = case("float64")
+    run = AdjointRun(make64, links64, steps=steps, window=window, checkpoint=checkpoint)
+    run.forward(1.0, G)
+    dU, dG = run.backward()
+    h = 1e-4
+    fd_u = (run.forward(1.0 + h, G) - run.forward(1.0 - h, G)) / (2 * h)
+    v = rng.standard_normal(G.shape) * p64.fluid
+    eps = h * np.abs(G).max()
+    fd_g = (run.forward(1.0, G + eps * v) - run.forward(1.0, G - eps * v)) / (2 * eps)
+    out["float64"] = {"dL_dU": dU, "fd_dL_dU": fd_u, "rel_err_U": abs(dU - fd_u) / abs(fd_u),
+                      "dL_dG_dot_v": float((dG * v).sum()), "fd_dL_dG_dot_v": fd_g,
+                      "rel_err_G": abs(float((dG * v).sum()) - fd_g) / abs(fd_g)}
+    out["float32_vs_float64_dU"] = abs(out["float32"]["dL_dU"] - dU) / abs(dU)
+    return out
+
+
+def batched_study(lbm, torch, steps: int = 640, separate_steps: int = 20):
+    """Batched configuration: 256 lid-driven cavities, sides U{64..512} (seeded), lid 0.1, Re U(100, 1000),
+    float32 TRT. Aggregate MLUPS of the persistent batched launch (CUDA graph, autotuned tile and grid)
+    against every domain launched on its own each step, host-driven and replayed from a CUDA graph.
+    """
+    from lbm_b200.batched import BatchedSolver, cavity_batch
+
+    params, sizes, _ = cavity_batch(lbm, count=256, n_min=64, n_max=512, seed=0)
+    batch = BatchedSolver(params)
+    nodes = batch.nodes
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        ev[0].record()
+        fn(k)
+        ev[1].record()
+        ev[1].synchronize()
+        return ev[0].elapsed_time(ev[1]) / k
+
+    batch.run(64)
+    ms_batched = timed(batch._advance, steps)
+    batch.run_separately(2)
+    ms_separate = timed(batch.run_separately, separate_steps)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        batch.run_separately(2)  # two steps: the buffers end where they started
+    graph.replay()
+    ms_separate_graph = timed(lambda k: [graph.replay() for _ in range(k // 2)], separate_steps)
+    batch.check_health()
+    return {"domains": len(params), "nodes": int(nodes), "side_min": int(sizes.min()), "side_max": int(sizes.max()),
+            "block": list(batch.block), "blocks": batch.blocks,
+            "batched_mlups": round(nodes / ms_batched / 1e3, 1),
+            "separate_host_launches_mlups": round(nodes / ms_separate / 1e3, 1),
+            "separate_graph_launches_mlups": round(nodes / ms_separate_graph / 1e3, 1),
+            "steps": {"batched": steps, "separate": separate_steps}}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -350,7 +464,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": warm, "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPE_TAG[args.storage], "data": "synthetic (analytic duct set-up, fluid at rest)",
         "config": workload_config(args),
-        "roofline": {"bound": "hbm", "kernel": f"lbm_bulk_kernel<D3Q19, {args.storage}, {args.variant}>",
+        "roofline": {"bound": "hbm", "kernel": step_kernel_name(args),
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_update": bpu, "copy_peak_in_run_gbs": round(copy_now, 1),
@@ -370,6 +484,12 @@ def run_ours(args, rank, world, local_rank):
         line["fp16_store"] = {"mlups": fp16["mlups"], "vs_fp32_mlups": round(fp16["mlups"] / study["float32"]["mlups"], 3),
                               "u_rel_l2_vs_f64": fp16["u_rel_l2_vs_f64"], "u_rel_max_vs_f64": fp16["u_rel_max_vs_f64"],
                               "steps": args.precision_steps}
+    if args.batched and world == 1:
+        torch.cuda.empty_cache()
+        line["batched"] = batched_study(lbm, torch)
+    if args.adjoint and world == 1:
+        torch.cuda.empty_cache()
+        line["adjoint"] = adjoint_study(lbm, torch)
     if not args.no_cpu_baseline and world == 1:
         mlups_cpu, done, dt = oracle_mlups(n, 8, 3, 1, budget=args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(mlups_cpu, 4), "unit": "MLUPS", "cores": 1, "kind": "port",

@@ -68,13 +68,24 @@ class AdjointRun:
 
     # ------------------------------------------------------------------ set-up
     def _setup(self, scale: float, G):
+        if self.solver is not None and self._scale == scale:
+            # same inlet scale, same rules and tables: only the force field changes
+            s = self.solver
+            field = np.zeros((s.lattice.d, *s.shape)) if G is None else np.asarray(G, dtype=np.float64)
+            s._force_field.copy_(s._upload_field(field.reshape(s.lattice.d, *s.shape)))
+            return
         params, d_rules = self.make_params(scale)
         if params.immersed is not None:
             raise ValueError("the adjoint supports walls, forces and link rules (no immersed bodies)")
         if params.dtype not in ("float32", "float64"):
             raise ValueError("the adjoint needs float32 or float64 storage (its recomputed forward must be exact)")
-        s = CudaSolver(params, variant="pull", block=self.block, force_field=G, graph=False, keep_zero_terms=True)
+        if G is None:
+            G = np.zeros((params.d, *params.shape))
+        # rule terms: those with a nonzero coefficient or a nonzero U-derivative
+        keep = None if d_rules is None else np.asarray(d_rules.values.coeff) != 0.0
+        s = CudaSolver(params, variant="pull", block=self.block, force_field=G, graph=True, keep_terms=keep)
         self.solver, self.params, self.d_rules = s, params, d_rules
+        self._scale = scale
         torch = s.torch
         probe = ForceProbe.build(params, self.links)
         comp = probe.compiled("pull")
@@ -192,7 +203,12 @@ class AdjointRun:
                N.ptr(out_slot), s._stream())
 
     def forward(self, scale: float = 1.0, G=None) -> float:
-        """Run T steps from rest; returns the loss (host float)."""
+        """Run T steps from rest; returns the loss (host float).
+
+        Steps between checkpoints that are outside the loss window replay the
+        solver's CUDA graphs; steps in the window run one by one, each followed
+        by the probe reduction of its value.
+        """
         import torch
 
         self._setup(float(scale), G)
@@ -203,23 +219,56 @@ class AdjointRun:
         self._u0 = torch.zeros((s.lattice.d, s.qstride), dtype=torch.float64, device=s.device)
         self._checkpoints = {}
         values = torch.zeros((M, s.lattice.d), dtype=torch.float64, device=s.device)
-        for t in range(T):
+        t = 0
+        while t < T:
             if t % K == 0:
                 self._checkpoints[t] = s._f.clone()
-            s._launch_pull()
+            stop = min((t // K + 1) * K, T)
             if t + 1 > T - M:
-                self._probe_value(values[t + 1 - (T - M + 1)])
+                for u in range(t, stop):
+                    s._launch_pull()
+                    self._probe_value(values[u + 1 - (T - M + 1)])
+                t = stop
+            else:
+                run = min(stop, T - M) - t
+                s._advance(run)
+                t += run
         self.loss = float(values[:, self.axis].sum().item()) / M
         return self.loss
 
     # ------------------------------------------------------------------ backward
+    def _capture(self, fn):
+        """A CUDA graph of the launches fn makes (fn computes its stream inside)."""
+        s = self.solver
+        torch = s.torch
+        stream = torch.cuda.Stream(s.device)
+        stream.wait_stream(torch.cuda.current_stream(s.device))
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            graph.capture_begin()
+            try:
+                fn()
+            finally:
+                graph.capture_end()
+        torch.cuda.current_stream(s.device).wait_stream(stream)
+        return graph
+
     def backward(self):
-        """(dL/dU, dL/dG (d, *shape) host float64) for the last forward()."""
+        """(dL/dU, dL/dG (d, *shape) host float64) for the last forward().
+
+        Segments of K steps, from the last: the forward states of a segment
+        are recomputed from its checkpoint into a ring of K buffers, then the
+        adjoint steps run backwards through them. Two rings alternate, so the
+        recomputation of the next (earlier) segment runs on its own stream
+        while the adjoint kernels sweep the current one. Full segments replay
+        CUDA graphs (the recomputation, and the adjoint steps per loss-source
+        scale); the first adjoint step and partial segments launch one by one.
+        """
         s = self.solver
         torch = s.torch
         T, M, K = self.steps, self.window, self.K
         q = s.lattice.q
-        ring = [torch.empty((q, s.qstride), dtype=s.t_store, device=s.device) for _ in range(K)]
+        rings = [[torch.empty((q, s.qstride), dtype=s.t_store, device=s.device) for _ in range(K)] for _ in range(2)]
         mu = [torch.empty((q, s.qstride), dtype=s.t_real, device=s.device) for _ in range(2)]
         self._force_grad.zero_()
         if self._rule_du is not None:
@@ -227,26 +276,87 @@ class AdjointRun:
         sp, adj = self._special_struct(), self._adj_struct()
         g, ph = N.C.byref(s.grid), N.C.byref(s.physics)
         launches = [N.Launch(self.block[0], self.block[1], m) for m in (N.LAUNCH_BULK, N.LAUNCH_BOUNDARY)]
-        stream = s._stream()
-        mu_next = None
-        cur = 0
-        for start in sorted(self._checkpoints, reverse=True):
-            stop = min(start + K, T)
-            # recompute f_start .. f_{stop-1} into the ring
-            ring[0].copy_(self._checkpoints[start])
-            for t in range(start, stop - 1):
-                s._f, s._f_next = ring[t - start], ring[t - start + 1]
+        f_saved = (s._f, s._f_next)
+        main = torch.cuda.current_stream(s.device)
+        rec_stream = torch.cuda.Stream(s.device)
+        adj_side = torch.cuda.Stream(s.device)
+
+        def recompute(ring, n):
+            for j in range(n - 1):
+                s._f, s._f_next = ring[j], ring[j + 1]
                 s._launch_pull()
+
+        def scale_of(t):
+            return 1.0 / M if t + 1 > T - M else 0.0
+
+        def adjoint_steps(ring, start, stop, cur, mu_next):
+            # bulk and boundary adjoint kernels touch disjoint nodes: the
+            # boundary one runs on a side stream, concurrently
+            here = torch.cuda.current_stream(s.device)
             for t in range(stop - 1, start - 1, -1):
-                scale = 1.0 / M if t + 1 > T - M else 0.0
                 out = mu[cur]
-                for lc in launches:
+                fork, join = torch.cuda.Event(), torch.cuda.Event()
+                fork.record(here)
+                adj_side.wait_event(fork)
+                for lc, stream in ((launches[1], adj_side), (launches[0], here)):
                     N.call("lbm_adjoint_step", g, ph, N.C.byref(sp), N.C.byref(adj), N.C.byref(lc),
-                           N.ptr(self._adj_kind), N.ptr(ring[t - start]), N.ptr(mu_next), N.ptr(out), scale, stream)
+                           N.ptr(self._adj_kind), N.ptr(ring[t - start]), N.ptr(mu_next), N.ptr(out), scale_of(t),
+                           stream.cuda_stream)
+                join.record(adj_side)
+                here.wait_event(join)
                 mu_next = out
                 cur ^= 1
+            return cur, mu_next
+
+        graphs = {}
+        starts = sorted(self._checkpoints, reverse=True)
+        ready = [None, None]  # recomputation of the ring finished
+        free = [None, None]   # adjoint steps done reading the ring
+
+        def launch_recompute(idx):
+            start = starts[idx]
+            n = min(start + K, T) - start
+            rid = idx & 1
+            with torch.cuda.stream(rec_stream):
+                if free[rid] is not None:
+                    rec_stream.wait_event(free[rid])
+                rings[rid][0].copy_(self._checkpoints[start])
+                if n == K:
+                    key = ("recompute", rid)
+                    if key not in graphs:
+                        graphs[key] = self._capture(lambda: recompute(rings[rid], K))
+                    graphs[key].replay()
+                else:
+                    recompute(rings[rid], n)
+                ready[rid] = torch.cuda.Event()
+                ready[rid].record(rec_stream)
+
+        launch_recompute(0)
+        mu_next = None
+        cur = 0
+        for idx, start in enumerate(starts):
+            if idx + 1 < len(starts):
+                launch_recompute(idx + 1)
+            rid = idx & 1
+            stop = min(start + K, T)
+            n = stop - start
+            main.wait_event(ready[rid])
+            scales = {scale_of(t) for t in range(start, stop)}
+            if n == K and mu_next is not None and len(scales) == 1:
+                key = ("adjoint", scales.pop(), cur, rid)
+                if key not in graphs:
+                    c0 = cur
+                    graphs[key] = self._capture(lambda: adjoint_steps(rings[rid], start, stop, c0, mu[c0 ^ 1]))
+                graphs[key].replay()
+                cur ^= K & 1
+                mu_next = mu[cur ^ 1]
+            else:
+                cur, mu_next = adjoint_steps(rings[rid], start, stop, cur, mu_next)
+            free[rid] = torch.cuda.Event()
+            free[rid].record(main)
+        s._f, s._f_next = f_saved
         N.call("lbm_adjoint_initial", g, ph, N.C.byref(sp), N.C.byref(adj), N.ptr(self._adj_kind), N.ptr(mu_next),
-               N.ptr(self._rho0), N.ptr(self._u0), 0.0, stream)
+               N.ptr(self._rho0), N.ptr(self._u0), 0.0, s._stream())
         dU = float(self._rule_du.sum().item()) if self._rule_du is not None else 0.0
         dG = s._from_pitched(self._force_grad).astype(np.float64)
         return dU, dG

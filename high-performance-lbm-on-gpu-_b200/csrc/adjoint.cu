@@ -160,9 +160,46 @@ struct AdjointKernel {
         finish(A, nd, s, lam);
     }
 
+    // Rule r and its U-derivative from one pass over the term loads:
+    // v = const + sum coeff f (as rule_value), d = dconst + sum dcoeff f in
+    // float64. Loads issued sixteen terms at a time (last batch predicated).
+    __device__ static __forceinline__ void rule_value_du(const AdjArgs& A, int r, R& v, double& d)
+    {
+        constexpr int B = 16;
+        const StepArgs& a = A.a;
+        const lbm_special_t& sp = a.sp;
+        const R* __restrict__ coeff = static_cast<const R*>(sp.term_coeff);
+        const R* __restrict__ dcoeff = static_cast<const R*>(A.adj.term_dcoeff);
+        const T* __restrict__ f = static_cast<const T*>(a.f_src);
+        v = static_cast<const R*>(sp.rule_const)[r];
+        d = (double)static_cast<const R*>(A.adj.rule_dconst)[r];
+        const int t1 = sp.term_start[r + 1];
+        for (int t = sp.term_start[r]; t < t1; t += B) {
+            int64_t slot[B];
+            R c[B], dc[B], val[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const bool in = t + k < t1;
+                slot[k] = in ? (int64_t)sp.term_dir[t + k] * a.qstride + sp.term_node[t + k] : 0;
+                c[k] = in ? coeff[t + k] : R(0);
+                dc[k] = in ? dcoeff[t + k] : R(0);
+            }
+#pragma unroll
+            for (int k = 0; k < B; ++k) val[k] = S::load(f + slot[k]);
+#pragma unroll
+            for (int k = 0; k < B; ++k)
+                if (t + k < t1) {
+                    v = v_fma(c[k], val[k], v);
+                    d += (double)dc[k] * (double)val[k];
+                }
+        }
+    }
+
     // Any fluid node that is not interior: bounce-back and wrap; for nodes of
     // the adjoint list (s_idx >= 0) also rules, rule-term and loss gathers.
-    __device__ static __forceinline__ void general(const AdjArgs& A, int64_t nd, int64_t s_idx)
+    // acc: this thread's column of a shared [Q][BOUNDARY_THREADS] array
+    // (boundary kernel; nullptr in the bulk kernel, which has no gathers).
+    __device__ static __forceinline__ void general(const AdjArgs& A, int64_t nd, int64_t s_idx, R* acc)
     {
         const StepArgs& a = A.a;
         const lbm_special_t& sp = a.sp;
@@ -203,54 +240,79 @@ struct AdjointKernel {
                     lam[i] = mn[L::opp(i) * qs + nd];
             }
         }
-        // rules replace bounce-back values in the forward gather
+        // rules replace bounce-back values in the forward gather; with a
+        // U-derivative the same term loads also give d(rule)/dU (dv)
+        const bool with_du = A.adj.rule_du != nullptr && A.adj.rule_dconst != nullptr;
+        double dv[Q];
+#pragma unroll
+        for (int j = 0; j < Q; ++j) dv[j] = 0.0;
         {
             uint32_t m = rmask;
             int r = rfirst;
-            const R* coeff = static_cast<const R*>(sp.term_coeff);
             while (m) {
                 const int i = __ffs(m) - 1;
                 m &= m - 1u;
-                R v = static_cast<const R*>(sp.rule_const)[r];
-                for (int t = sp.term_start[r]; t < sp.term_start[r + 1]; ++t)
-                    v += coeff[t] * S::load(f + (int64_t)sp.term_dir[t] * qs + sp.term_node[t]);
+                R v;
+                double d = 0.0;
+                if (with_du)
+                    rule_value_du(A, r, v, d);
+                else
+                    v = StepKernel<L, ST, LBM_PULL>::rule_value(a, r);
                 ++r;
 #pragma unroll
                 for (int j = 0; j < Q; ++j)
-                    if (j == i) s[j] = v;
+                    if (j == i) {
+                        s[j] = v;
+                        dv[j] = d;
+                    }
             }
         }
-        // rule-term and loss gathers into lambda
+        // rule-term and loss gathers into lambda, accumulated per direction in
+        // shared memory (a runtime direction index; in registers it would be
+        // a select over all Q directions per entry), then added to lambda
         if (s_idx >= 0) {
+            constexpr int BT = BOUNDARY_THREADS;
+#pragma unroll
+            for (int j = 0; j < Q; ++j) acc[j * BT] = R(0);
+            // entries sixteen at a time: metadata, then the mu values
+            constexpr int B = 16;
             const R* gc = static_cast<const R*>(A.adj.gather_coeff);
             const R scale = R(A.loss_scale);
-            for (int e = A.adj.gather_start[s_idx]; e < A.adj.gather_start[s_idx + 1]; ++e) {
-                const int64_t slot = A.adj.gather_slot[e];
-                R v;
-                if (slot >= 0)
-                    v = mn != nullptr ? gc[e] * mn[slot] : R(0);
-                else
-                    v = gc[e] * scale;
-                const int k = A.adj.gather_dir[e];
+            const int e1 = A.adj.gather_start[s_idx + 1];
+            for (int e0 = A.adj.gather_start[s_idx]; e0 < e1; e0 += B) {
+                int64_t slot[B];
+                int dir[B];
+                R c[B], val[B];
 #pragma unroll
-                for (int j = 0; j < Q; ++j)
-                    if (j == k) lam[j] += v;
+                for (int k = 0; k < B; ++k) {
+                    const bool in = e0 + k < e1;
+                    slot[k] = in ? A.adj.gather_slot[e0 + k] : -1;
+                    dir[k] = in ? A.adj.gather_dir[e0 + k] : 0;
+                    c[k] = in ? gc[e0 + k] : R(0);
+                }
+#pragma unroll
+                for (int k = 0; k < B; ++k) val[k] = (slot[k] >= 0 && mn != nullptr) ? mn[slot[k]] : R(0);
+#pragma unroll
+                for (int k = 0; k < B; ++k)
+                    if (e0 + k < e1) acc[dir[k] * BT] += slot[k] >= 0 ? c[k] * val[k] : c[k] * scale;
             }
+#pragma unroll
+            for (int j = 0; j < Q; ++j) lam[j] += acc[j * BT];
         }
         finish(A, nd, s, lam);
         // d rule value / dU, weighted by mu of the ruled direction
-        if (A.adj.rule_du != nullptr && A.adj.rule_dconst != nullptr && rmask) {
+        if (with_du && rmask) {
             const R* mu = static_cast<const R*>(A.mu_out) + nd;
-            const R* dcoeff = static_cast<const R*>(A.adj.term_dcoeff);
             uint32_t m = rmask;
             int r = rfirst;
             while (m) {
                 const int i = __ffs(m) - 1;
                 m &= m - 1u;
-                double v = (double)static_cast<const R*>(A.adj.rule_dconst)[r];
-                for (int t = sp.term_start[r]; t < sp.term_start[r + 1]; ++t)
-                    v += (double)dcoeff[t] * (double)S::load(f + (int64_t)sp.term_dir[t] * qs + sp.term_node[t]);
-                A.adj.rule_du[r] += (double)mu[i * qs] * v;
+                double d = 0.0;
+#pragma unroll
+                for (int j = 0; j < Q; ++j)
+                    if (j == i) d = dv[j];
+                A.adj.rule_du[r] += (double)mu[i * qs] * d;
                 ++r;
             }
         }
@@ -269,14 +331,16 @@ __global__ void __launch_bounds__(256) lbm_adjoint_bulk_kernel(const AdjArgs A)
     if (k == KIND_FLUID)
         AdjointKernel<L, ST>::interior(A, nd);
     else if (!(k & (KIND_SOLID | KIND_SPECIAL)))
-        AdjointKernel<L, ST>::general(A, nd, -1);
+        AdjointKernel<L, ST>::general(A, nd, -1, nullptr);
 }
 
 template <class L, int ST>
 __global__ void __launch_bounds__(256, 1) lbm_adjoint_boundary_kernel(const AdjArgs A)
 {
+    using R = typename Storage<ST>::R;
+    __shared__ R acc[L::Q * BOUNDARY_THREADS];
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (s < A.a.sp.n_special) AdjointKernel<L, ST>::general(A, A.a.sp.node[s], s);
+    if (s < A.a.sp.n_special) AdjointKernel<L, ST>::general(A, A.a.sp.node[s], s, acc + threadIdx.x);
 }
 
 template <class L, int ST>
@@ -289,7 +353,8 @@ int adjoint_step(const AdjArgs& A, int mode, int tile_x, int tile_y, cudaStream_
         lbm_adjoint_bulk_kernel<L, ST><<<grid, dim3(tile_x, tile_y), 0, s>>>(A);
     }
     if (mode != LBM_LAUNCH_BULK && a.sp.n_special > 0)
-        lbm_adjoint_boundary_kernel<L, ST><<<(unsigned)((a.sp.n_special + 127) / 128), 128, 0, s>>>(A);
+        lbm_adjoint_boundary_kernel<L, ST>
+            <<<(unsigned)((a.sp.n_special + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS), BOUNDARY_THREADS, 0, s>>>(A);
     return launch_status();
 }
 

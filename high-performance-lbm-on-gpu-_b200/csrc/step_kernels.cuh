@@ -41,21 +41,52 @@ struct StepKernel {
     using R = typename S::R;
     static constexpr int Q = L::Q;
 
+    // Rule r: const + sum_t coeff[t] f*_{dir[t]}(node[t]), summed in term
+    // order with explicit fma. Terms are taken sixteen at a time (a partial
+    // last batch is predicated): all term metadata, then all values, so a
+    // Zou-He rule -- it combines the 14 known populations of its node --
+    // costs two memory round trips instead of two per term.
     __device__ static __forceinline__ R rule_value(const StepArgs& a, int r)
     {
+        constexpr int B = 16;
         const lbm_special_t& sp = a.sp;
         const R* __restrict__ coeff = static_cast<const R*>(sp.term_coeff);
         R v = static_cast<const R*>(sp.rule_const)[r];
         const int t1 = sp.term_start[r + 1];
         if (VAR == LBM_PULL) {
             const T* __restrict__ f = static_cast<const T*>(a.f_src);
-            for (int t = sp.term_start[r]; t < t1; ++t) {
-                const int64_t slot = (int64_t)sp.term_dir[t] * a.qstride + sp.term_node[t];
-                v += coeff[t] * S::load(f + slot);
+            for (int t = sp.term_start[r]; t < t1; t += B) {
+                int64_t slot[B];
+                R c[B], val[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const bool in = t + k < t1;
+                    slot[k] = in ? (int64_t)sp.term_dir[t + k] * a.qstride + sp.term_node[t + k] : 0;
+                    c[k] = in ? coeff[t + k] : R(0);
+                }
+#pragma unroll
+                for (int k = 0; k < B; ++k) val[k] = S::load(f + slot[k]);
+#pragma unroll
+                for (int k = 0; k < B; ++k)
+                    if (t + k < t1) v = v_fma(c[k], val[k], v);
             }
         } else {
             const R* __restrict__ ex = static_cast<const R*>(sp.export_in);
-            for (int t = sp.term_start[r]; t < t1; ++t) v += coeff[t] * ex[sp.term_export[t]];
+            for (int t = sp.term_start[r]; t < t1; t += B) {
+                int e[B];
+                R c[B], val[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const bool in = t + k < t1;
+                    e[k] = in ? sp.term_export[t + k] : 0;
+                    c[k] = in ? coeff[t + k] : R(0);
+                }
+#pragma unroll
+                for (int k = 0; k < B; ++k) val[k] = ex[e[k]];
+#pragma unroll
+                for (int k = 0; k < B; ++k)
+                    if (t + k < t1) v = v_fma(c[k], val[k], v);
+            }
         }
         return v;
     }
@@ -402,6 +433,12 @@ __global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
     }
 }
 
+// Boundary launches: one warp per block, so that a few thousand special
+// nodes -- each a long chain of dependent loads (rule terms) -- spread over
+// every SM instead of filling a few (measured 52 -> see the boundary-kernel
+// profile; 256-thread blocks put an 8,900-node list on 35 of the 148 SMs).
+constexpr int BOUNDARY_THREADS = 32;
+
 template <class L, int ST, int VAR>
 static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cudaStream_t stream)
 {
@@ -410,8 +447,8 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
     const unsigned gy = (unsigned)((a.ny + tile_y - 1) / tile_y);
     if (mode == LBM_LAUNCH_BOUNDARY) {
         if (a.sp.n_special <= 0) return LBM_OK;
-        const int64_t blocks = (a.sp.n_special + 255) / 256;
-        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY><<<(unsigned)blocks, 256, 0, stream>>>(a);
+        const int64_t blocks = (a.sp.n_special + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS;
+        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY><<<(unsigned)blocks, BOUNDARY_THREADS, 0, stream>>>(a);
     } else if (mode == LBM_LAUNCH_BULK) {
         if (a.nz > 65535) return LBM_ERR_INVALID;
         if constexpr (VAR == LBM_PULL && has_vec<ST>()) {

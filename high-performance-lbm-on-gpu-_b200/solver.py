@@ -165,7 +165,7 @@ class CudaSolver(Solver):
 
     def __init__(self, params, variant: str = "pull", block=DEFAULT_BLOCK, force_field=None,
                  graph: bool = True, device=None, pitch: int | None = None, launch: str = "split",
-                 keep_zero_terms: bool = False):
+                 keep_zero_terms: bool = False, keep_terms=None):
         if variant not in VARIANTS:
             raise ValueError(f"unknown CUDA variant {variant!r}; choose from {VARIANTS}")
         if launch not in ("fused", "split"):
@@ -216,6 +216,9 @@ class CudaSolver(Solver):
         self.grid = N.Grid(N.LATTICE_CODE[lattice.name], N.STORAGE_CODE[self.storage], nx, ny, nz, self.pitch, self.qstride)
         self.launch_mode = launch
         self.keep_zero_terms = bool(keep_zero_terms)
+        # optional mask (rules x terms, in the rules' order) of zero-coefficient
+        # terms to keep: the adjoint keeps those whose U-derivative is nonzero
+        self._keep_terms = None if keep_terms is None else np.asarray(keep_terms, dtype=bool)
         self._launches = {m: N.Launch(bx, by, m) for m in N.LAUNCH_MODES}
         self.block = (bx, by)
 
@@ -312,8 +315,11 @@ class CudaSolver(Solver):
             order = np.lexsort((direction, node))
             node, direction = node[order], direction[order]
             coeff, tdir, tnode, const = coeff[order], tdir[order], tnode[order], const[order]
-            # keep_zero_terms: a fixed term structure (the adjoint aligns derivatives with it)
+            # keep_zero_terms: a fixed term structure; keep_terms: zero terms that
+            # another table (the adjoint's derivatives) aligns with
             live = np.ones_like(coeff, dtype=bool) if self.keep_zero_terms else coeff != 0.0
+            if self._keep_terms is not None:
+                live |= self._keep_terms[order]
             self._rule_order, self._rule_live = order, live
             start = np.zeros(len(node) + 1, dtype=np.int64)
             np.cumsum(live.sum(axis=1), out=start[1:])
@@ -472,7 +478,8 @@ class CudaSolver(Solver):
             sp = self._special_struct()
             self._native("lbm_export_prime", N.C.byref(self.grid), N.C.byref(sp), N.ptr(self._f), N.LAYOUT_AA_ODD,
                          N.ptr(self._export_cur), self._stream())
-        self._graphs.clear()
+            # captured graphs baked the export buffers' order in
+            self._graphs.clear()
 
     def _natural_populations(self):
         """Device tensor (q, qstride) of f*_i in natural order, compute dtype."""
