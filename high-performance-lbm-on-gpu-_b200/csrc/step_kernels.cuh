@@ -435,8 +435,8 @@ __global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
 
 // Boundary launches: one warp per block, so that a few thousand special
 // nodes -- each a long chain of dependent loads (rule terms) -- spread over
-// every SM instead of filling a few (measured 52 -> see the boundary-kernel
-// profile; 256-thread blocks put an 8,900-node list on 35 of the 148 SMs).
+// every SM instead of filling a few (256-thread blocks put an 8,900-node
+// list on 35 of the 148 SMs).
 constexpr int BOUNDARY_THREADS = 32;
 
 template <class L, int ST, int VAR>

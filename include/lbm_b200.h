@@ -63,12 +63,15 @@ typedef struct lbm_physics {
     const void* force_field; /* real[d][qstride] per-node body force added to force[], or NULL */
     const uint32_t* solid_nbr; /* per node: bit i set where x - c_i is solid (lbm_classify); read only
                                   at fluid nodes that are not interior */
-    uint32_t* round_seed;  /* float16/bfloat16 storage (required there, ignored otherwise): two uint32
-                              slots holding the step counter of the stochastic rounding of stored
-                              populations. A step reads slot p and its bulk (or fused) launch writes
-                              slot 1 - p with the count + 1, where p = (f_src > f_dst) for
-                              lbm_step_pull and p = parity for lbm_step_aa. Set both slots to the same
-                              value (0) whenever the populations are set. */
+    uint32_t* round_seed;  /* float16/bfloat16 storage (required there, ignored otherwise): three
+                              uint32 slots in device memory. Slots 0 and 1 hold the step counter of
+                              the stochastic rounding of stored populations: a step reads slot p and
+                              its bulk (or fused) launch writes slot 1 - p with the count + 1, where
+                              p = (f_src > f_dst) for lbm_step_pull and p = parity for lbm_step_aa.
+                              Set both to the same value (0) whenever the populations are set.
+                              Slot 2 is a status word, zeroed by the caller: the TMA-staged pull
+                              kernel sets bit 0 when a block gave up waiting for its staged loads
+                              (bounded wait), in which case the step's output is incomplete. */
 } lbm_physics_t;
 
 /* Nodes updated by the boundary warps, and the link rules they apply.
@@ -110,7 +113,13 @@ typedef struct lbm_special {
  *   LBM_LAUNCH_BOUNDARY the boundary warps only (1D grid over the list).
  * BULK and BOUNDARY touch disjoint nodes and may run concurrently; together
  * they are one time step. Split launches let the bulk kernel keep its small
- * register budget. */
+ * register budget. For float16/bfloat16 storage, LBM_LAUNCH_BULK of
+ * lbm_step_pull takes the TMA-staged kernel (persistent blocks over 2-row
+ * tiles, tile_x/tile_y unused) when nx is a power of two in [16, 256], pitch
+ * is a multiple of 16, f_src and kind are 16-byte aligned, force_field is
+ * NULL and round_seed is given; otherwise a kernel with two nodes per thread
+ * (pitch and qstride even, no force_field), else one node per thread. All
+ * three give the same bits. */
 enum { LBM_LAUNCH_FUSED = 0, LBM_LAUNCH_BULK = 1, LBM_LAUNCH_BOUNDARY = 2 };
 typedef struct lbm_launch {
     int32_t tile_x;   /* multiple of 32 */
@@ -326,7 +335,8 @@ typedef struct lbm_batch {
     const uint8_t* kind;           /* kind pool (domain i at kind_offset) */
     const uint32_t* solid_nbr;     /* solid-neighbour pool, same offsets as kind */
     const void* wall_u;            /* wall pool (compute type) or NULL */
-    uint32_t* round_seed;          /* as lbm_physics_t.round_seed, one counter for the whole batch */
+    uint32_t* round_seed;          /* slots 0 and 1 as lbm_physics_t.round_seed, one counter for the
+                                      whole batch (slot 2 is not used here) */
 } lbm_batch_t;
 
 /* One two-lattice pull step of every domain of the batch -- the batched
