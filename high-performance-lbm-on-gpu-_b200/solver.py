@@ -124,6 +124,10 @@ class Solver(ABC):
 # ---------------------------------------------------------------------------- device tables
 
 
+PINNED_READOUT_BYTES = 1 << 30
+"""Largest host readout (macroscopic fields, populations) copied through page-locked memory."""
+
+
 @dataclass
 class _SpecialTables:
     """Device form of the boundary-warp work list (see ``lbm_special_t``)."""
@@ -273,10 +277,24 @@ class CudaSolver(Solver):
         return out.reshape(*lead, self.qstride)
 
     def _from_pitched(self, t):
-        """Device tensor (..., qstride) -> host array (..., *shape)."""
+        """Device tensor (..., qstride) -> host array (..., *shape).
+
+        Readouts up to PINNED_READOUT_BYTES land in page-locked host memory
+        (torch's caching host allocator reuses the block once the returned
+        array is dropped), which the copy engine fills at full link speed; a
+        pageable destination goes through a staging buffer at a fraction of it.
+        """
+        torch = self.torch
         lead = t.shape[:-1]
         view = t.reshape(*lead, *self.shape[:-1], self.pitch)[..., : self.shape[-1]]
-        return view.contiguous().cpu().numpy()
+        if self.pitch != self.shape[-1]:
+            view = view.contiguous()
+        if view.numel() * view.element_size() > PINNED_READOUT_BYTES:
+            return view.cpu().numpy()
+        host = torch.empty(view.shape, dtype=view.dtype, pin_memory=True)
+        host.copy_(view, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return host.numpy()
 
     def _upload_field(self, host):
         return self._to_pitched(np.asarray(host, dtype=np.float64), self.t_real)
@@ -616,8 +634,8 @@ class CudaSolver(Solver):
         """rho and u on the host (reference ``solver.py:209-221``)."""
         torch = self.torch
         d = self.lattice.d
-        rho = torch.empty(self.qstride, dtype=self.t_real, device=self.device)
-        u = torch.empty((d, self.qstride), dtype=self.t_real, device=self.device)
+        fields = torch.empty((d + 1, self.qstride), dtype=self.t_real, device=self.device)
+        rho, u = fields[0], fields[1:]
         local_nodes = local = None
         n_local = 0
         if self._ibm is not None:
@@ -626,9 +644,8 @@ class CudaSolver(Solver):
             n_local = self._ibm.tables.n_nodes
         self._native("lbm_macroscopic", N.C.byref(self.grid), N.C.byref(self.physics), N.ptr(self._kind), N.ptr(self._f),
                      self._layout_code, N.ptr(local_nodes), N.ptr(local), n_local, N.ptr(rho), N.ptr(u), self._stream())
-        rho_h = self._from_pitched(rho)
-        u_h = self._from_pitched(u)
-        return MacroscopicFields(rho=rho_h, u=tuple(u_h[a] for a in range(d)), solid=np.array(self._solid_host))
+        host = self._from_pitched(fields)  # one copy for rho and u
+        return MacroscopicFields(rho=host[0], u=tuple(host[1 + a] for a in range(d)), solid=np.array(self._solid_host))
 
     def _device_slots(self, compiled):
         slots = np.asarray(compiled.slots, dtype=np.int64)
