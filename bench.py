@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched-cavities study (aggregate MLUPS against separate launches)")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the Taylor-Green and cylinder configuration studies")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the adjoint-configuration study (forward/backward cost and finite differences)")
     ap.add_argument("--precision-steps", type=int, default=5000,
@@ -333,6 +335,108 @@ def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: 
     return out
 
 
+def tgv_study(lbm, torch, n: int = 512, steps: int = 1000):
+    """Taylor-Green configuration: D2Q9 TRT n x n periodic, tau = 0.8, float32, u0 = 0.01 (sin kx cos ky,
+    -cos kx sin ky), k = 2 pi / n. MLUPS of `steps` steps (CUDA events; the 2 x 19 MB lattice stays in L2)
+    and the decay of the velocity amplitude against exp(-2 nu k^2 t), nu = (tau - 1/2)/3.
+    """
+    tau = 0.8
+    k = 2 * math.pi / n
+    y, x = np.mgrid[0:n, 0:n]
+    ux = 0.01 * np.sin(k * x) * np.cos(k * y)
+    uy = -0.01 * np.cos(k * x) * np.sin(k * y)
+    params = lbm.SimulationParams(nx=n, ny=n, tau=tau, collision="trt", dtype="float32")
+    s = lbm.make_solver(params, backend="cuda-naive")
+    s.initialize(1.0, ux, uy)
+    s._advance(s.GRAPH_CHUNK)  # graph capture
+    s.initialize(1.0, ux, uy)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    s._advance(steps)
+    b.record()
+    b.synchronize()
+    s.time_step = steps
+    s._check_health()
+    f = s.macroscopic()
+    amp = float((f.u[0] * ux).sum() / (ux * ux).sum())
+    exact = math.exp(-2 * (tau - 0.5) / 3 * k * k * steps)
+    return {"config": f"D2Q9 TRT {n}x{n} periodic, tau={tau}, float32, {steps} steps",
+            "mlups": round(n * n * steps / (a.elapsed_time(b) / 1e3) / 1e6, 1),
+            "amplitude": amp, "amplitude_exact": exact, "amplitude_rel_err": abs(amp - exact) / exact}
+
+
+def cylinder_params(lbm, method: str, nx: int = 880, ny: int = 164, u_max: float = 0.05, iterations: int = 3):
+    """Cylinder configuration: D2Q9 channel nx x ny, walls at y = 0 and ny - 1, circle D = 40 at (200, 82),
+    parabolic Zou-He inflow (U_max 0.05, profile as the reference's 2D-2 builder), outlet rho = 1, Re = 100
+    (tau from nu = U_mean D / Re), float32; the body as Bouzidi links or as an immersed boundary."""
+    lattice = lbm.D2Q9
+    height = ny - 2
+    yc = np.arange(ny) - 0.5
+    profile = np.where((yc > 0) & (yc < height), 4.0 * u_max * yc * (height - yc) / height**2, 0.0)
+    inflow = np.stack([profile, np.zeros(ny)])
+    solid = np.zeros((ny, nx), dtype=bool)
+    solid[0, :] = solid[-1, :] = True
+    body = lbm.circle(200.0, 82.0, 20.0)
+    immersed = links = None
+    if method == "ibm":
+        immersed = lbm.ImmersedBoundary.from_ball(body, spacing=1.0, iterations=iterations)
+    else:
+        solid |= lbm.voxelize(body, solid.shape)
+    solid, rules = lbm.open_channel(lattice, solid, inflow)
+    if method == "bouzidi":
+        links = lbm.wall_links(lattice, body, solid)
+        rules = lbm.LinkRules.concat(rules, lbm.bouzidi_rules(lattice, links, solid))
+    u_mean = 2.0 * u_max / 3.0
+    tau = 3.0 * (u_mean * 40.0 / 100.0) + 0.5
+    params = lbm.SimulationParams(nx=nx, ny=ny, tau=tau, collision="trt", solid=solid, dtype="float32",
+                                  link_rules=rules, immersed=immersed)
+    return params, links, u_mean
+
+
+def cylinder_study(lbm, torch, steps: int = 40000, every: int = 100):
+    """Cylinder configuration, Bouzidi and immersed boundary: `steps` steps from rest through the public run
+    loop, drag and lift sampled every `every` steps in float64 (force probe / immersed-body force), as
+    C = F / (0.5 U_mean^2 D). MLUPS of the whole run (wall clock, samples included) and of the steps alone
+    (CUDA events, no sampling); C_D mean and C_L range over the last quarter of the run.
+    """
+    out = {}
+    for method in ("bouzidi", "ibm"):
+        params, links, u_mean = cylinder_params(lbm, method)
+        s = lbm.make_solver(params, backend="cuda-naive")
+        probe = lbm.ForceProbe.build(params, links) if links is not None else None
+        scale = 0.5 * u_mean**2 * 40.0
+        samples = []
+
+        def sample(solver):
+            fx, fy = probe.evaluate(solver) if probe is not None else solver.immersed_force
+            samples.append((solver.time_step, fx / scale, fy / scale))
+
+        s._advance(s.GRAPH_CHUNK)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s._advance(2000)
+        b.record()
+        b.synchronize()
+        ms_step = a.elapsed_time(b) / 2000
+        s.initialize()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run(steps, every=every, callback=sample, check_every=steps)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        tail = np.array([v for v in samples if v[0] > 0.75 * steps])
+        nodes = params.nx * params.ny
+        out[method] = {"mlups_run": round(nodes * steps / wall / 1e6, 1),
+                       "mlups_steps": round(nodes / ms_step / 1e3, 1), "us_per_step": round(ms_step * 1e3, 2),
+                       "cd_mean": float(tail[:, 1].mean()), "cl_min": float(tail[:, 2].min()),
+                       "cl_max": float(tail[:, 2].max()), "samples": len(samples)}
+        del s
+        torch.cuda.empty_cache()
+    out["config"] = (f"D2Q9 880x164 channel, cylinder D=40 at (200, 82), Zou-He parabolic inflow U_max=0.05, Re=100, "
+                     f"float32, {steps} steps, C_D/C_L every {every} steps (tail: last quarter)")
+    return out
+
+
 def batched_study(lbm, torch, steps: int = 640, separate_steps: int = 20):
     """Batched configuration: 256 lid-driven cavities, sides U{64..512} (seeded), lid 0.1, Re U(100, 1000),
     float32 TRT. Aggregate MLUPS of the persistent batched launch (CUDA graph, autotuned tile and grid)
@@ -485,6 +589,10 @@ def run_ours(args, rank, world, local_rank):
         line["fp16_store"] = {"mlups": fp16["mlups"], "vs_fp32_mlups": round(fp16["mlups"] / study["float32"]["mlups"], 3),
                               "u_rel_l2_vs_f64": fp16["u_rel_l2_vs_f64"], "u_rel_max_vs_f64": fp16["u_rel_max_vs_f64"],
                               "steps": args.precision_steps}
+    if args.configs and world == 1:
+        torch.cuda.empty_cache()
+        line["tgv"] = tgv_study(lbm, torch)
+        line["cylinder"] = cylinder_study(lbm, torch)
     if args.batched and world == 1:
         torch.cuda.empty_cache()
         line["batched"] = batched_study(lbm, torch)

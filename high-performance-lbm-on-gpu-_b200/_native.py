@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -73,7 +73,7 @@ class Ibm(C.Structure):
 class Adjoint(C.Structure):
     _fields_ = [
         ("gather_start", vp), ("gather_dir", vp), ("gather_slot", vp), ("gather_coeff", vp), ("rule_dconst", vp),
-        ("term_dcoeff", vp), ("rule_du", vp), ("force_grad", vp),
+        ("term_dcoeff", vp), ("rule_du", vp), ("force_grad", vp), ("local_force_grad", vp),
     ]
 
 
@@ -115,6 +115,8 @@ _SIGNATURES = {
     "lbm_ibm_moments": [P(Grid), P(Physics), P(Ibm), vp, i32, vp],
     "lbm_ibm_iteration": [P(Grid), P(Ibm), i32, vp, vp, vp],
     "lbm_ibm_body_force": [P(Grid), P(Ibm), i32, vp, vp],
+    "lbm_ibm_adjoint_iteration": [P(Grid), P(Ibm), vp, vp, i32, C.c_double, vp, vp, vp],
+    "lbm_ibm_adjoint_moments": [P(Grid), P(Ibm), vp, vp, vp],
     "lbm_kernel_resources": [i32, i32, i32, vp],
 }
 EXPORTED = (*_SIGNATURES, "lbm_last_cuda_error", "lbm_abi_version")

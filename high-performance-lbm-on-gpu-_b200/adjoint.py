@@ -5,6 +5,9 @@ of ``steps`` steps (the momentum-exchange drag, ``forces.ForceProbe``)::
 
     L(U, G) = (1/M) sum_{t = T-M+1..T} D(f_t),   D = probe force . e_axis
 
+or, for an immersed body and no probe, its body-force component averaged over
+the last ``window`` steps (``lbm_ibm_body_force``).
+
 Parameters: a per-node Guo force field G (d, *shape) and, optionally, the
 scale U of the Zou-He inlet velocity (rules and their exact derivative from
 ``open_boundaries.zou_he_inlet_derivative``).
@@ -18,6 +21,11 @@ adjoint kernel per step (``lbm_adjoint_step``: transposed streaming +
 transposed TRT/Guo collision + transposed link rules + loss source) runs
 backwards through them; a closing kernel adds the initial-state term. The
 gradient w.r.t. U accumulates per rule in float64 and is summed at the end.
+With an immersed body, every backward step first recomputes the step's
+multi-direct passes from its state (the node force enters the collision of the
+stencil nodes), and after the adjoint kernel runs the passes in reverse
+(``lbm_ibm_adjoint_iteration``) and adds the resulting dL/d(streamed
+populations) at the stencil nodes to mu (``lbm_ibm_adjoint_moments``).
 
 ``LbmDragLoss`` wraps forward/backward as a ``torch.autograd.Function``.
 """
@@ -48,7 +56,8 @@ class AdjointRun:
     Args:
         make_params: callable (scale U) -> (params, d_rules); ``params.link_rules``
             and ``d_rules`` row/term aligned (``aligned_rules``). ``d_rules`` may be None.
-        links: wall links of the body whose force is the loss.
+        links: wall links of the body whose force is the loss, or None: the loss is
+            the force on the immersed body (``params.immersed``).
         steps, window: run length T and averaging window M.
         axis: force component (0 = drag along x).
         checkpoint: steps between checkpoints K.
@@ -75,8 +84,8 @@ class AdjointRun:
             s._force_field.copy_(s._upload_field(field.reshape(s.lattice.d, *s.shape)))
             return
         params, d_rules = self.make_params(scale)
-        if params.immersed is not None:
-            raise ValueError("the adjoint supports walls, forces and link rules (no immersed bodies)")
+        if self.links is None and params.immersed is None:
+            raise ValueError("without wall links the loss is the immersed body's force: params.immersed is None")
         if params.dtype not in ("float32", "float64"):
             raise ValueError("the adjoint needs float32 or float64 storage (its recomputed forward must be exact)")
         if G is None:
@@ -87,15 +96,70 @@ class AdjointRun:
         self.solver, self.params, self.d_rules = s, params, d_rules
         self._scale = scale
         torch = s.torch
-        probe = ForceProbe.build(params, self.links)
-        comp = probe.compiled("pull")
-        self.probe = probe
-        slots, coeff, const, (rows, terms) = s._affine_tensors(comp)
-        self._probe_t = (slots, coeff, const, rows, terms)
-        self._probe_w = torch.from_numpy(np.ascontiguousarray(probe.weight)).to(s.device)
-        self._partial = torch.empty(((rows + 255) // 256) * s.lattice.d, dtype=torch.float64, device=s.device)
-        self._counter = torch.zeros(1, dtype=torch.int32, device=s.device)
-        self._build_adjoint_tables(comp, probe.weight[:, self.axis])
+        self.probe = comp = None
+        if self.links is not None:
+            probe = ForceProbe.build(params, self.links)
+            comp = probe.compiled("pull")
+            self.probe = probe
+            slots, coeff, const, (rows, terms) = s._affine_tensors(comp)
+            self._probe_t = (slots, coeff, const, rows, terms)
+            self._probe_w = torch.from_numpy(np.ascontiguousarray(probe.weight)).to(s.device)
+            self._partial = torch.empty(((rows + 255) // 256) * s.lattice.d, dtype=torch.float64, device=s.device)
+            self._counter = torch.zeros(1, dtype=torch.int32, device=s.device)
+        self._ibm_adj = self._build_ibm_adjoint() if s._ibm is not None else None
+        self._build_adjoint_tables(comp, None if self.probe is None else self.probe.weight[:, self.axis])
+
+    def _build_ibm_adjoint(self):
+        """Scratch of the immersed-boundary adjoint: a private copy of the pass buffers (the recomputed
+        forward of one step), every pass's node force, the ping-pong node-force adjoints and the
+        float64 moment adjoints."""
+        s = self.solver
+        torch = s.torch
+        ibm = s._ibm
+        tab = ibm.tables
+        rules = self.params.link_rules
+        if rules is not None and len(rules):
+            if np.intersect1d(np.asarray(rules.node), tab.nodes).size:
+                raise ValueError("the adjoint needs the immersed-boundary stencil nodes free of link rules")
+        d, n, dev, real = s.lattice.d, tab.n_nodes, s.device, s.t_real
+        st = {
+            "rho": torch.zeros(n, dtype=real, device=dev),
+            "u_star": torch.zeros((d, n), dtype=real, device=dev),
+            "marker_force": torch.zeros((tab.iterations, d, tab.n_markers), dtype=real, device=dev),
+            "force": [torch.zeros((d, n), dtype=real, device=dev) for _ in range(tab.iterations)],
+            "adj": [torch.zeros((d, n), dtype=real, device=dev) for _ in range(2)],
+            "moments": torch.zeros((1 + d, n), dtype=torch.float64, device=dev),
+        }
+        base = ibm.struct
+        st["struct"] = N.Ibm(base.n_nodes, base.n_markers, base.stencil_size, base.node, base.stencil, base.weight,
+                             base.area, base.inv_start, base.inv_marker, base.inv_weight, N.ptr(st["rho"]),
+                             N.ptr(st["u_star"]), N.ptr(st["marker_force"]))
+        return st
+
+    def _ibm_recompute(self, f, stream):
+        """The multi-direct passes of the step from state f, keeping every pass's node force."""
+        s, st = self.solver, self._ibm_adj
+        g = N.C.byref(s.grid)
+        N.call("lbm_ibm_moments", g, N.C.byref(s.physics), N.C.byref(st["struct"]), N.ptr(f), N.LAYOUT_PULL, stream)
+        for it, out in enumerate(st["force"]):
+            fin = st["force"][it - 1] if it else None
+            N.call("lbm_ibm_iteration", g, N.C.byref(st["struct"]), it, N.ptr(fin), N.ptr(out), stream)
+
+    def _ibm_reverse(self, mu, body_scale, stream):
+        """Passes in reverse from dL/d(node force) (written by the adjoint step), then add the moment
+        adjoints into mu at the stencil nodes."""
+        s, st = self.solver, self._ibm_adj
+        g, ib = N.C.byref(s.grid), N.C.byref(st["struct"])
+        axis = self.axis if self.probe is None else -1
+        cur = 0
+        K = len(st["force"])
+        for j in range(K - 1, -1, -1):
+            prev = st["force"][j - 1] if j else None
+            out = st["adj"][cur ^ 1] if j else None
+            N.call("lbm_ibm_adjoint_iteration", g, ib, N.ptr(prev), N.ptr(st["adj"][cur]), axis, body_scale,
+                   N.ptr(out), N.ptr(st["moments"]), stream)
+            cur ^= 1
+        N.call("lbm_ibm_adjoint_moments", g, ib, N.ptr(st["moments"]), N.ptr(mu), stream)
 
     def _build_adjoint_tables(self, comp, w_axis):
         """Adjoint special list: forward special nodes + rule-term nodes + probe nodes, with gather tables.
@@ -120,13 +184,15 @@ class AdjointRun:
                     if a != 0.0:
                         entries.setdefault(int(s._pitched(np.array([y]))[0]), []).append((int(k), mu_slot, float(a)))
         # loss gradient dD/df at probe slots (layout pull = natural)
-        slots = np.asarray(comp.slots)
-        coeff = np.asarray(comp.coeff)
-        for r in range(slots.shape[0]):
-            for t in range(slots.shape[1]):
-                if coeff[r, t] != 0.0 and w_axis[r] != 0.0:
-                    k, y = divmod(int(slots[r, t]), n)
-                    entries.setdefault(int(s._pitched(np.array([y]))[0]), []).append((k, -1, float(w_axis[r] * coeff[r, t])))
+        if comp is not None:
+            slots = np.asarray(comp.slots)
+            coeff = np.asarray(comp.coeff)
+            for r in range(slots.shape[0]):
+                for t in range(slots.shape[1]):
+                    if coeff[r, t] != 0.0 and w_axis[r] != 0.0:
+                        k, y = divmod(int(slots[r, t]), n)
+                        entries.setdefault(int(s._pitched(np.array([y]))[0]), []).append(
+                            (k, -1, float(w_axis[r] * coeff[r, t])))
         base = s._special.tensors.get("node")
         base_nodes = base.cpu().numpy() if base is not None else np.zeros(0, dtype=np.int64)
         extra = np.array(sorted(entries), dtype=np.int64)
@@ -137,9 +203,11 @@ class AdjointRun:
         t = s._special.tensors
         rule_mask = np.zeros(ns, dtype=np.uint32)
         rule_first = np.zeros(ns, dtype=np.int32)
+        force_slot = np.full(ns, -1, dtype=np.int32)
         if base_nodes.size:
             rule_mask[pos] = t["rule_mask"].cpu().numpy().view(np.uint32)
             rule_first[pos] = t["rule_first"].cpu().numpy()
+            force_slot[pos] = t["force_slot"].cpu().numpy()
         starts = np.zeros(ns + 1, dtype=np.int64)
         dirs, gslots, gcoef = [], [], []
         for i, node in enumerate(nodes.tolist()):
@@ -153,7 +221,7 @@ class AdjointRun:
             "node": torch.from_numpy(nodes).to(dev),
             "rule_mask": torch.from_numpy(rule_mask.view(np.int32)).to(dev),
             "rule_first": torch.from_numpy(rule_first).to(dev),
-            "force_slot": torch.full((ns,), -1, dtype=torch.int32, device=dev),
+            "force_slot": torch.from_numpy(force_slot).to(dev),
             "zero": torch.zeros(max(ns, 1), dtype=torch.int32, device=dev),
             "gather_start": torch.from_numpy(starts.astype(np.int32)).to(dev),
             "gather_dir": torch.from_numpy(np.asarray(dirs, dtype=np.int32)).to(dev),
@@ -181,22 +249,31 @@ class AdjointRun:
         s = self.solver
         t, f = self._adj_t, s._special
         g = t.get
+        st = self._ibm_adj
+        local = st["force"][-1] if st is not None else None  # the node force of the recomputed last pass
         return N.Special(
             int(t["node"].numel()), N.ptr(g("node")), N.ptr(g("rule_mask")), N.ptr(g("rule_first")),
             N.ptr(g("force_slot")), N.ptr(g("zero")), N.ptr(g("zero")), f.n_rules, f.n_terms,
             N.ptr(f.tensors.get("term_start")), N.ptr(f.tensors.get("rule_const")), N.ptr(f.tensors.get("term_dir")),
-            N.ptr(f.tensors.get("term_node")), None, N.ptr(f.tensors.get("term_coeff")), None, 0, 0, None, None,
+            N.ptr(f.tensors.get("term_node")), None, N.ptr(f.tensors.get("term_coeff")), N.ptr(local),
+            f.n_local if st is not None else 0, 0, None, None,
         )
 
     def _adj_struct(self):
         t = self._adj_t
+        st = self._ibm_adj
         return N.Adjoint(N.ptr(t["gather_start"]), N.ptr(t["gather_dir"]), N.ptr(t["gather_slot"]),
                          N.ptr(t["gather_coeff"]), N.ptr(t.get("rule_dconst")), N.ptr(t.get("term_dcoeff")),
-                         N.ptr(self._rule_du), N.ptr(self._force_grad))
+                         N.ptr(self._rule_du), N.ptr(self._force_grad), N.ptr(st["adj"][0] if st is not None else None))
 
     # ------------------------------------------------------------------ forward
     def _probe_value(self, out_slot):
         s = self.solver
+        if self.probe is None:
+            ibm = s._ibm
+            N.call("lbm_ibm_body_force", N.C.byref(s.grid), N.C.byref(ibm.struct), ibm.tables.iterations,
+                   N.ptr(out_slot), s._stream())
+            return
         slots, coeff, const, rows, terms = self._probe_t
         N.call("lbm_affine_reduce", s.grid.storage, N.ptr(s._f), N.ptr(slots), N.ptr(coeff), N.ptr(const),
                N.ptr(self._probe_w), rows, terms, s.lattice.d, N.ptr(self._partial), N.ptr(self._counter),
@@ -207,7 +284,8 @@ class AdjointRun:
 
         Steps between checkpoints that are outside the loss window replay the
         solver's CUDA graphs; steps in the window run one by one, each followed
-        by the probe reduction of its value.
+        by the probe reduction of its value (or the immersed body's force of
+        that step).
         """
         import torch
 
@@ -293,17 +371,22 @@ class AdjointRun:
             # bulk and boundary adjoint kernels touch disjoint nodes: the
             # boundary one runs on a side stream, concurrently
             here = torch.cuda.current_stream(s.device)
+            ibm_loss = self.probe is None
             for t in range(stop - 1, start - 1, -1):
                 out = mu[cur]
                 fork, join = torch.cuda.Event(), torch.cuda.Event()
                 fork.record(here)
                 adj_side.wait_event(fork)
+                if self._ibm_adj is not None:  # the boundary kernel reads the step's node force
+                    self._ibm_recompute(ring[t - start], adj_side.cuda_stream)
                 for lc, stream in ((launches[1], adj_side), (launches[0], here)):
                     N.call("lbm_adjoint_step", g, ph, N.C.byref(sp), N.C.byref(adj), N.C.byref(lc),
-                           N.ptr(self._adj_kind), N.ptr(ring[t - start]), N.ptr(mu_next), N.ptr(out), scale_of(t),
-                           stream.cuda_stream)
+                           N.ptr(self._adj_kind), N.ptr(ring[t - start]), N.ptr(mu_next), N.ptr(out),
+                           0.0 if ibm_loss else scale_of(t), stream.cuda_stream)
                 join.record(adj_side)
                 here.wait_event(join)
+                if self._ibm_adj is not None:
+                    self._ibm_reverse(out, scale_of(t) if ibm_loss else 0.0, here.cuda_stream)
                 mu_next = out
                 cur ^= 1
             return cur, mu_next

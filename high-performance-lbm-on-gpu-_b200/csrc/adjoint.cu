@@ -127,11 +127,22 @@ struct AdjointKernel {
         }
     }
 
-    __device__ static __forceinline__ void finish(const AdjArgs& A, int64_t nd, const R (&s)[Q], R (&lam)[Q])
+    // s_idx >= 0: node of the special list; its force slot (immersed-boundary
+    // stencil nodes) adds the recomputed node force, and dL/dF there goes to
+    // local_force_grad for the immersed-boundary adjoint.
+    __device__ static __forceinline__ void finish(const AdjArgs& A, int64_t nd, const R (&s)[Q], R (&lam)[Q],
+                                                  int64_t s_idx = -1)
     {
         const StepArgs& a = A.a;
         R F[3], g[3];
         force_at(a, nd, F);
+        const int fs = s_idx >= 0 && a.sp.force_slot != nullptr ? a.sp.force_slot[s_idx] : -1;
+        if (fs >= 0) {
+            const R* lf = static_cast<const R*>(a.sp.local_force);
+            const int64_t n = a.sp.n_local;
+#pragma unroll
+            for (int c = 0; c < L::D; ++c) F[c] += lf[c * n + fs];
+        }
         collide_vjp<L, R>(s, lam, R(a.wp), R(a.wm), F, g);
         R* mu = static_cast<R*>(A.mu_out) + nd;
 #pragma unroll
@@ -140,6 +151,11 @@ struct AdjointKernel {
             R* fg = static_cast<R*>(A.adj.force_grad) + nd;
 #pragma unroll
             for (int c = 0; c < L::D; ++c) fg[c * a.qstride] += g[c];
+        }
+        if (fs >= 0 && A.adj.local_force_grad != nullptr) {
+            R* lg = static_cast<R*>(A.adj.local_force_grad);
+#pragma unroll
+            for (int c = 0; c < L::D; ++c) lg[c * (int64_t)a.sp.n_local + fs] = g[c];
         }
     }
 
@@ -299,7 +315,7 @@ struct AdjointKernel {
 #pragma unroll
             for (int j = 0; j < Q; ++j) lam[j] += acc[j * BT];
         }
-        finish(A, nd, s, lam);
+        finish(A, nd, s, lam, s_idx);
         // d rule value / dU, weighted by mu of the ruled direction
         if (with_du && rmask) {
             const R* mu = static_cast<const R*>(A.mu_out) + nd;
@@ -468,6 +484,7 @@ static bool make_adj(AdjArgs& A, const lbm_grid_t* g, const lbm_physics_t* p, co
     else
         memset(&a.sp, 0, sizeof(a.sp));
     if (a.sp.n_special > 0 && (!adj->gather_start || !a.sp.node || !a.sp.rule_mask || !a.sp.rule_first)) return false;
+    if (a.sp.n_local > 0 && a.sp.n_special > 0 && (!a.sp.force_slot || !a.sp.local_force)) return false;
     A.adj = *adj;
     A.mu_next = mu_next;
     A.mu_out = mu_out;

@@ -135,6 +135,128 @@ __global__ void ibm_body_force_kernel(const lbm_ibm_t ib, int iterations, double
     }
 }
 
+// ---------------------------------------------------------------- adjoint
+// Reverse of one pass, node-centric and deterministic like the forward pass:
+// node n walks its (marker l, w_ln) list and, per marker, recomputes the
+// forward rho_l and U_l of the pass and the adjoint of F_l,
+//   Fbar_l = sum_s w_ls adj_in(m(l,s)) - body_scale e_axis,
+// from which (F_l = -2 dA_l rho_l U_l, U_l = sum_s w_ls (u*_s + Fp_s / (2 rho_s)))
+//   d/dFp_n : -dA_l rho_l w_ln / rho_n
+//   d/du*_n : -2 dA_l rho_l w_ln
+//   d/drho_n: -2 dA_l w_ln U_l + dA_l rho_l w_ln Fp_n / rho_n^2   (through rho_l and Fp_n / (2 rho_n))
+// applied to Fbar_l. Float64 throughout.
+template <class L, int ST>
+__global__ void ibm_adjoint_iteration_kernel(const lbm_ibm_t ib, const typename Storage<ST>::R* __restrict__ fprev,
+                                             const typename Storage<ST>::R* __restrict__ adj_in, int axis,
+                                             double body_scale, typename Storage<ST>::R* __restrict__ adj_out,
+                                             double* __restrict__ madj)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ib.n_nodes) return;
+    const int nn = ib.n_nodes;
+    const R* __restrict__ rho = (const R*)ib.rho;
+    const R* __restrict__ us = (const R*)ib.u_star;
+    const R* __restrict__ wgt = (const R*)ib.weight;
+    const R* __restrict__ area = (const R*)ib.area;
+    const R* __restrict__ invw = (const R*)ib.inv_weight;
+    const double rho_n = (double)rho[n];
+    double o[D], ub[D], rb = 0.0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) o[a] = ub[a] = 0.0;
+    for (int p = ib.inv_start[n]; p < ib.inv_start[n + 1]; ++p) {
+        const int l = ib.inv_marker[p];
+        const int* st = ib.stencil + (int64_t)l * ib.stencil_size;
+        const R* wl = wgt + (int64_t)l * ib.stencil_size;
+        double rho_l = 0.0, U[D], Fb[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) U[a] = Fb[a] = 0.0;
+        for (int s = 0; s < ib.stencil_size; ++s) {
+            const int m = st[s];
+            const double w = (double)wl[s];
+            const double rm = (double)rho[m];
+            rho_l += w * rm;
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                double u = (double)us[a * nn + m];
+                if (fprev != nullptr) u += (double)fprev[a * nn + m] / (2.0 * rm);
+                U[a] += w * u;
+                Fb[a] += w * (double)adj_in[a * nn + m];
+            }
+        }
+        if (axis >= 0 && axis < D) Fb[axis] -= body_scale;
+        const double wn = (double)invw[p], dA = (double)area[l];
+        const double c = dA * rho_l * wn;
+        double UF = 0.0, PF = 0.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            o[a] += c * Fb[a];
+            ub[a] -= 2.0 * c * Fb[a];
+            UF += U[a] * Fb[a];
+            if (fprev != nullptr) PF += Fb[a] * (double)fprev[a * nn + n];
+        }
+        rb += -2.0 * dA * wn * UF + c * PF / (rho_n * rho_n);
+    }
+    if (adj_out != nullptr) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) adj_out[a * nn + n] = (R)((double)adj_in[a * nn + n] - o[a] / rho_n);
+    }
+    madj[n] += rb;
+#pragma unroll
+    for (int a = 0; a < D; ++a) madj[(int64_t)(1 + a) * nn + n] += ub[a];
+}
+
+// rho = 1 + sum_k s_k, u* = (j + F_uniform / 2) / rho, j = sum_k c_k s_k:
+//   d/ds_k = rho_bar - u*_bar . u* / rho + c_k . u*_bar / rho
+template <class L, int ST>
+__global__ void ibm_adjoint_moments_kernel(const lbm_grid_t g, const lbm_ibm_t ib, double* __restrict__ madj,
+                                           typename Storage<ST>::R* __restrict__ mu)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ib.n_nodes) return;
+    const int nn = ib.n_nodes;
+    const R* __restrict__ us = (const R*)ib.u_star;
+    const double rho = (double)((const R*)ib.rho)[n];
+    double rb = madj[n], jb[3] = {0.0, 0.0, 0.0};
+    madj[n] = 0.0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const double ub = madj[(int64_t)(1 + a) * nn + n];
+        madj[(int64_t)(1 + a) * nn + n] = 0.0;
+        rb -= ub * (double)us[a * nn + n] / rho;
+        jb[a] = ub / rho;
+    }
+    const int64_t nd = ib.node[n];
+#pragma unroll
+    for (int k = 0; k < L::Q; ++k) {
+        const double v = rb + L::cx(k) * jb[0] + L::cy(k) * jb[1] + L::cz(k) * jb[2];
+        mu[(int64_t)k * g.qstride + nd] += (R)v;
+    }
+}
+
+template <class L, int ST>
+int ibm_adjoint_iteration(const lbm_grid_t& g, const lbm_ibm_t& ib, const void* fprev, const void* adj_in, int axis,
+                          double body_scale, void* adj_out, double* madj, cudaStream_t s)
+{
+    using R = typename Storage<ST>::R;
+    if (ib.n_nodes <= 0) return LBM_OK;
+    ibm_adjoint_iteration_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(
+        ib, (const R*)fprev, (const R*)adj_in, axis, body_scale, (R*)adj_out, madj);
+    return launch_status();
+}
+
+template <class L, int ST>
+int ibm_adjoint_moments(const lbm_grid_t& g, const lbm_ibm_t& ib, double* madj, void* mu, cudaStream_t s)
+{
+    using R = typename Storage<ST>::R;
+    if (ib.n_nodes <= 0) return LBM_OK;
+    ibm_adjoint_moments_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(g, ib, madj, (R*)mu);
+    return launch_status();
+}
+
 template <class L, int ST>
 int ibm_moments(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, const void* f, int layout, cudaStream_t s)
 {
@@ -194,4 +316,20 @@ extern "C" int lbm_ibm_body_force(const lbm_grid_t* g, const lbm_ibm_t* ib, int3
 {
     if (!ibm_ok(g, ib) || !out || iterations < 1) return LBM_ERR_INVALID;
     LBM_DISPATCH(g->lattice, g->storage, ibm_body_force, *g, *ib, iterations, out, (cudaStream_t)stream);
+}
+
+extern "C" int lbm_ibm_adjoint_iteration(const lbm_grid_t* g, const lbm_ibm_t* ib, const void* force_prev,
+                                         const void* adj_in, int32_t axis, double body_scale, void* adj_out,
+                                         double* moment_adj, lbm_stream_t stream)
+{
+    if (!ibm_ok(g, ib) || !adj_in || !moment_adj || adj_in == adj_out) return LBM_ERR_INVALID;
+    LBM_DISPATCH(g->lattice, g->storage, ibm_adjoint_iteration, *g, *ib, force_prev, adj_in, axis, body_scale, adj_out,
+                 moment_adj, (cudaStream_t)stream);
+}
+
+extern "C" int lbm_ibm_adjoint_moments(const lbm_grid_t* g, const lbm_ibm_t* ib, double* moment_adj, void* mu,
+                                       lbm_stream_t stream)
+{
+    if (!ibm_ok(g, ib) || !moment_adj || !mu) return LBM_ERR_INVALID;
+    LBM_DISPATCH(g->lattice, g->storage, ibm_adjoint_moments, *g, *ib, moment_adj, mu, (cudaStream_t)stream);
 }

@@ -162,7 +162,9 @@ class CudaSolver(Solver):
         params: a ``SimulationParams`` (this package's or the reference's).
         variant: ``"pull"`` (two lattices) or ``"aa"`` (in place, steps in pairs).
         block: bulk tile (x, y) in threads; x a multiple of 32, at most 256 threads.
-        force_field: optional per-node Guo force (d, *shape) added to the uniform force.
+        force_field: optional per-node Guo force (d, *shape) added to the uniform force (and,
+            at immersed-boundary stencil nodes, to the node force; the immersed-boundary
+            moments u* use the uniform force only, as the reference's).
         graph: capture chunks of steps in CUDA graphs (saves launch latency on small grids).
         device: CUDA device (default: current).
     """
@@ -245,8 +247,6 @@ class CudaSolver(Solver):
         if params.immersed is not None:
             from .ibm import build_tables
 
-            if force_field is not None:
-                raise ValueError("a per-node force field cannot be combined with an immersed body")
             self._ibm = _IbmState(self, build_tables(params.immersed, lattice, np.asarray(params.solid)))
         self._solid_host = np.asarray(params.solid, dtype=bool)
         self._special = self._build_special(params)
@@ -486,6 +486,28 @@ class CudaSolver(Solver):
         if self._f_next is not None:
             self._f_next.copy_(self._f)
         self._after_state_change()
+
+    def save_checkpoint(self, path) -> None:
+        """Population-exact snapshot on disk (``.npz``): the populations in natural order, shape
+        (q, *shape), in the compute type (exact for every storage format), the time step and the step
+        counter of the stochastic rounding of 16-bit storage, so that a restored run continues bit
+        for bit (``load_checkpoint``)."""
+        counter = int(self._seed[:2].cpu().numpy().view(np.uint32).max())
+        np.savez(path, populations=self.populations(), time_step=np.int64(self.time_step),
+                 round_step=np.uint32(counter), dtype=np.str_(self.params.dtype), shape=np.asarray(self.shape),
+                 lattice=np.str_(self.lattice.name))
+
+    def load_checkpoint(self, path) -> None:
+        """Restore a ``save_checkpoint`` snapshot of a run with the same lattice, shape and storage."""
+        with np.load(path) as z:
+            if (tuple(int(v) for v in z["shape"]) != tuple(self.shape) or str(z["dtype"]) != self.params.dtype
+                    or str(z["lattice"]) != self.lattice.name):
+                raise ValueError(f"checkpoint of a {z['lattice']} {tuple(z['shape'])} {z['dtype']} run; this solver "
+                                 f"is {self.lattice.name} {tuple(self.shape)} {self.params.dtype}")
+            self.set_populations(z["populations"])
+            counter = np.array([int(z["round_step"])], dtype=np.uint32).view(np.int32)[0]
+            self._seed[:2].fill_(int(counter))
+            self.time_step = int(z["time_step"])
 
     def _after_state_change(self):
         self._seed[:2].zero_()

@@ -267,6 +267,30 @@ int lbm_ibm_iteration(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iter
 int lbm_ibm_body_force(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iterations, double* out,
                        lbm_stream_t stream);
 
+/* Reverse of one multi-direct pass (no counterpart in the reference, which has
+ * no adjoint). With the forward quantities of the step recomputed in ibm
+ * (rho, u_star, and force_prev = the node force entering the pass, NULL for
+ * the first), adj_in = dL/d(node force after the pass), and the body-force
+ * loss term dL/dF_l[axis] = -body_scale (axis < 0: none), node-centric:
+ *   Fbar_l  = sum_s w_ls adj_in(m(l,s)) - body_scale e_axis
+ *   adj_out(n)     = adj_in(n) - (1/rho_n) sum_l dA_l rho_l w_ln Fbar_l   (if adj_out != NULL)
+ *   moment_adj[1+a](n) += sum_l -2 dA_l rho_l w_ln Fbar_l[a]             (dL/du*)
+ *   moment_adj[0](n)   += sum_l w_ln (-2 dA_l U_l . Fbar_l)
+ *                         + dA_l rho_l w_ln (Fbar_l . force_prev(n)) / rho_n^2   (dL/drho)
+ * moment_adj: double[1 + d][n_nodes], accumulated over the passes. */
+int lbm_ibm_adjoint_iteration(const lbm_grid_t* grid, const lbm_ibm_t* ibm, const void* force_prev,
+                              const void* adj_in, int32_t axis, double body_scale, void* adj_out,
+                              double* moment_adj, lbm_stream_t stream);
+
+/* Closing part of the immersed-boundary adjoint (no counterpart in the
+ * reference): dL/d(streamed populations) at the stencil nodes from moment_adj,
+ *   mu[k](n) += rho_bar_n + c_k . u*_bar_n / rho_n,
+ *   rho_bar_n = moment_adj[0](n) - u*_bar_n . u*_n / rho_n,
+ * added into mu (real[Q][qstride], the adjoint of the streamed state written
+ * by lbm_adjoint_step); moment_adj is then zeroed for the next step. */
+int lbm_ibm_adjoint_moments(const lbm_grid_t* grid, const lbm_ibm_t* ibm, double* moment_adj, void* mu,
+                            lbm_stream_t stream);
+
 /* ---- adjoint (reverse mode) of the two-lattice step ---------------------- */
 
 /* Extra tables of the adjoint step, per node of the adjoint special list (the
@@ -283,6 +307,9 @@ typedef struct lbm_adjoint {
     const void* term_dcoeff;       /* real[n_terms]: d coeff / dU aligned with the rule terms */
     double* rule_du;               /* double[n_rules] accumulator: sum over steps of mu_j * d rule value / dU */
     void* force_grad;              /* real[d][qstride] accumulator of dL/dG, or NULL */
+    void* local_force_grad;        /* real[d][n_local]: dL/dF at each special node with a force slot
+                                      (sp->force_slot >= 0, the immersed-boundary stencil nodes, whose
+                                      collision adds sp->local_force), written by every step, or NULL */
 } lbm_adjoint_t;
 
 /* One backward step of the two-lattice pull scheme, fused:

@@ -6,9 +6,14 @@ for the loss
 
     L = (1/M) sum_{t = T-M+1..T} D(f_t),   D(f) = sum_r weight[r, axis] (const_r + sum coeff f[slot])
 
-(a momentum-exchange force component, ``src/lbm/forces.py:98-103``) with
-respect to the per-node Guo force field G and the inlet-speed scale U of
-Zou-He rules whose derivative is given.
+(a momentum-exchange force component, ``src/lbm/forces.py:98-103``), or
+for an immersed body the mean of its body force component over the last M
+steps (``src/lbm/ibm.py:189-214``), with respect to the per-node Guo force
+field G and the inlet-speed scale U of Zou-He rules whose derivative is given.
+The immersed-boundary force enters the collision of its stencil nodes and
+depends on the streamed populations there; its vector-Jacobian product is
+taken by complex steps through the oracle's own multi-direct passes
+(``lbm_oracle._Ibm.force_from_moments``), one step per moment input.
 
 Independent of the CUDA adjoint by construction: the collision Jacobian is
 taken by complex-step differentiation of the oracle's own ``collide``
@@ -48,7 +53,8 @@ class OracleAdjoint:
     Args:
         params: float64 parameters (rules included).
         probe: (slots, coeff, constant) of the force probe in the reference layout,
-            ``weight`` (n_rows, d) and the force ``axis``.
+            ``weight`` (n_rows, d) and the force ``axis``; probe None: the loss is
+            the immersed body's force component ``axis`` (``weight`` unused).
         window: number M of final steps averaged in the loss.
         force_field: (d, *shape) per-node force (the parameter G).
         d_rules: derivative of ``params.link_rules`` w.r.t. U, same rows and
@@ -64,12 +70,17 @@ class OracleAdjoint:
         self.solid = np.asarray(params.solid, dtype=bool)
         self.fluid = ~self.solid
         self.G = np.asarray(force_field, dtype=np.float64).reshape(self.d, *self.shape)
-        slots, coeff, const = probe
-        w = np.asarray(weight, dtype=np.float64)[:, axis]
         self.window = int(window)
+        self.axis = int(axis)
         self.dD = np.zeros(self.lattice.q * self.n)
-        np.add.at(self.dD, np.asarray(slots).ravel(), (w[:, None] * np.asarray(coeff)).ravel())
-        self.probe = (np.asarray(slots), np.asarray(coeff), np.asarray(const), w)
+        self.probe = None
+        if probe is not None:
+            slots, coeff, const = probe
+            w = np.asarray(weight, dtype=np.float64)[:, axis]
+            np.add.at(self.dD, np.asarray(slots).ravel(), (w[:, None] * np.asarray(coeff)).ravel())
+            self.probe = (np.asarray(slots), np.asarray(coeff), np.asarray(const), w)
+        elif params.immersed is None:
+            raise ValueError("without a force probe the loss is the immersed body's force: params.immersed is None")
         self.src = _pull_sources(self.lattice, self.solid)
         rules = params.link_rules
         self.rules = None
@@ -112,15 +123,36 @@ class OracleAdjoint:
             self.solver.step()
             self.states.append(self.solver.populations())
             if t > steps - self.window:
-                total += self.loss_of(self.states[-1])
+                if self.probe is None:
+                    total += float(self.solver.ibm.body_force[self.axis])
+                else:
+                    total += self.loss_of(self.states[-1])
         self.steps = steps
         return total / self.window
 
-    def _vjp_collide(self, s, lam):
+    def _vjp_ibm(self, rho, j, a_bar, b_bar):
+        """(rho_bar, j_bar) at the stencil nodes from the adjoints of the node force (d, n) and body force (d,)."""
+        ibm = self.solver.ibm
+        n = rho.size
+        jj = np.stack(j).astype(np.complex128)
+        r0 = rho.astype(np.complex128)
+        bar = np.zeros((1 + self.d, n))
+        for m in range(1 + self.d):
+            for i in range(n):
+                r, jv = r0.copy(), jj.copy()
+                if m == 0:
+                    r[i] += 1j * H
+                else:
+                    jv[m - 1, i] += 1j * H
+                force, body = ibm.force_from_moments(r, list(jv))
+                bar[m, i] = (a_bar * force.imag).sum() / H + float(b_bar @ body.imag) / H
+        return bar[0], bar[1:]
+
+    def _vjp_collide(self, s, lam, force=None):
         """mu = J_s^T lam and g = J_F^T lam at every node, by complex steps."""
         q, d = self.lattice.q, self.d
         wp, wm = self.params.relaxation_rates
-        force = self._force()
+        force = self._force() if force is None else force
         mu = np.zeros_like(s)
         for k in range(q):
             z = s.astype(np.complex128)
@@ -141,10 +173,21 @@ class OracleAdjoint:
         dG = np.zeros((self.d, *self.shape))
         dU = 0.0
         fluid = self.fluid
+        ibm = self.solver.ibm
         for t in range(T - 1, -1, -1):
             f_t = self.states[t]
             s = self._streamed(f_t)
-            mu, g = self._vjp_collide(s, lam)
+            force = None
+            if ibm is not None:
+                rho_n, j_n = ibm.moments(f_t)
+                field, _ = ibm.force_from_moments(rho_n, j_n)
+                force = []
+                for a, fa in enumerate(self._force()):
+                    full = np.broadcast_to(np.asarray(fa, dtype=np.float64), self.shape).copy()
+                    full.reshape(-1)[ibm.nodes] += field[a]
+                    force.append(full)
+                force = tuple(force)
+            mu, g = self._vjp_collide(s, lam, force)
             mu = np.where(fluid, mu, 0.0)
             dG += np.where(fluid, g, 0.0)
             new = np.zeros(q * n)
@@ -164,6 +207,16 @@ class OracleAdjoint:
                     dU += float(mu_flat[target] @ dvals)
             else:
                 np.add.at(new, self.src.reshape(-1), mu_flat)
+            if ibm is not None:
+                # the node force depends on the streamed populations at the stencil nodes
+                a_bar = g.reshape(self.d, -1)[:, ibm.nodes]
+                b_bar = np.zeros(self.d)
+                if self.probe is None and t >= T - M:
+                    b_bar[self.axis] = 1.0 / M
+                rho_bar, j_bar = self._vjp_ibm(rho_n, j_n, a_bar, b_bar)
+                for k in range(q):
+                    s_bar = rho_bar + sum(int(ibm.c[k, a]) * j_bar[a] for a in range(self.d) if ibm.c[k, a])
+                    np.add.at(new, k * n + ibm.sources[k], s_bar)
             lam = new.reshape(q, *self.shape)
             if t > T - M:
                 lam = lam + self.dD.reshape(q, *self.shape) / M

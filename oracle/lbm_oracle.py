@@ -198,6 +198,13 @@ def _roma(r):
     return np.where(a <= 0.5, inner, np.where(a <= 1.5, outer, 0.0))
 
 
+def _bincount(index, weights, n):
+    """np.bincount with real or complex weights (complex: real and imaginary parts separately)."""
+    if np.iscomplexobj(weights):
+        return np.bincount(index, weights=weights.real, minlength=n) + 1j * np.bincount(index, weights=weights.imag, minlength=n)
+    return np.bincount(index, weights=weights, minlength=n)
+
+
 class _Ibm:
     """Direct-forcing IBM state (``ibm.py:123-214``), reference layout only."""
 
@@ -223,13 +230,21 @@ class _Ibm:
         self.c = np.asarray(lattice.c)
         self.body_force = np.zeros(d)
 
-    def force_field(self, f):
+    def moments(self, f):
+        """rho and j (d, n) of the streamed populations at the stencil nodes (``ibm.py:160-173``)."""
         q = self.sources.shape[0]
-        n = self.nodes.size
         streamed = f.reshape(q, -1)[np.arange(q)[:, None], self.sources]  # (q, n)
         drho = streamed.sum(axis=0)
         rho = 1.0 + drho
         j = [sum(self.c[k, a] * streamed[k] for k in range(q) if self.c[k, a]) for a in range(self.d)]
+        return rho, j
+
+    def force_from_moments(self, rho, j):
+        """Multi-direct passes (``ibm.py:189-214``): node force (d, n) and body force (d,).
+
+        Complex inputs are allowed (the adjoint differentiates this by complex steps).
+        """
+        n = self.nodes.size
         u_star = np.stack([(j[a] + 0.5 * self.uniform[a]) / rho for a in range(self.d)])
         rho_marker = (self.weights * rho[self.inverse]).sum(axis=1)
         force = np.zeros((self.d, n), dtype=u_star.dtype)
@@ -242,8 +257,11 @@ class _Ibm:
             total = total + f_marker.sum(axis=1)
             spread = (self.weights[None] * f_marker[:, :, None]).reshape(self.d, -1)
             for a in range(self.d):
-                force[a] = force[a] + np.bincount(flat_inv, weights=spread[a], minlength=n)
-        self.body_force = -total
+                force[a] = force[a] + _bincount(flat_inv, spread[a], n)
+        return force, -total
+
+    def force_field(self, f):
+        force, self.body_force = self.force_from_moments(*self.moments(f))
         return force
 
 

@@ -147,3 +147,114 @@ def test_torch_autograd_function():
     dU, dG = run.backward()
     assert U.grad.item() == pytest.approx(dU, rel=1e-14)
     np.testing.assert_allclose(G.grad.numpy(), dG, rtol=1e-14)
+
+
+# ---------------------------------------------------------------- immersed bodies
+
+
+def ibm_channel(d, dtype="float64", with_bouzidi=False):
+    """Zou-He channel with an immersed body (3 multi-direct passes); optionally also a Bouzidi body."""
+    if d == 2:
+        lat, (nx, ny) = lbm.D2Q9, (20, 12)
+        solid = lbm.channel_walls(nx, ny)
+        inflow = np.zeros((2, ny))
+        inflow[0, 1:-1] = 0.04
+        ball = lbm.circle(7.3, 5.6, 2.1)
+        wall_body = lbm.circle(15.2, 6.1, 1.8)
+        sizes = {"nx": nx, "ny": ny}
+    else:
+        lat, (nx, ny, nz) = lbm.D3Q19, (16, 11, 11)
+        solid = lbm.duct_walls(nx, ny, nz)
+        inflow = np.zeros((3, nz, ny))
+        inflow[0, 1:-1, 1:-1] = 0.04
+        ball = lbm.sphere(6.4, 5.3, 5.1, 1.7)
+        wall_body = lbm.sphere(11.6, 5.2, 5.4, 1.6)
+        sizes = {"nx": nx, "ny": ny, "nz": nz}
+    if with_bouzidi:
+        solid = solid | lbm.voxelize(wall_body, solid.shape)
+    body = lbm.ImmersedBoundary.from_ball(ball, spacing=1.0, iterations=3)
+
+    def make(scale):
+        s2, rules, d_rules = lbm.zou_he_inlet_derivative(lat, solid, scale * inflow)
+        all_rules, all_d = rules, d_rules
+        if with_bouzidi:
+            links = lbm.wall_links(lat, wall_body, s2)
+            all_rules, all_d = aligned_rules(rules, d_rules, lbm.bouzidi_rules(lat, links, s2))
+        p = lbm.SimulationParams(**sizes, tau=0.6, collision="trt", solid=s2, dtype=dtype, link_rules=all_rules,
+                                 immersed=body)
+        return p, all_d
+
+    p, _ = make(1.0)
+    links = lbm.wall_links(lat, wall_body, p.solid) if with_bouzidi else None
+    return make, links, p
+
+
+def oracle_ibm_gradients(make, links, G, steps, window):
+    p, d_rules = make(1.0)
+    if links is None:
+        adj = OracleAdjoint(p, None, None, 0, window, G, d_rules)
+    else:
+        probe = lbm.ForceProbe.build(p, links)
+        comp = probe.compiled("reference")
+        adj = OracleAdjoint(p, (comp.slots, comp.coeff, comp.constant), probe.weight, 0, window, G, d_rules)
+    loss = adj.forward(steps)
+    dU, dG = adj.backward()
+    return loss, dU, dG
+
+
+@pytest.mark.parametrize("d,with_bouzidi", [(2, False), (3, False), (2, True)],
+                         ids=["2d-body-force", "3d-body-force", "2d-probe-with-immersed-body"])
+def test_immersed_body_adjoint_matches_the_numpy_adjoint(d, with_bouzidi):
+    """Loss: the immersed body's drag (or a Bouzidi body's probe drag with the immersed body in the flow)."""
+    make, links, p = ibm_channel(d, "float64", with_bouzidi)
+    rng = np.random.default_rng(4)
+    G = 1e-5 * rng.standard_normal((p.d, *p.shape)) * p.fluid
+    steps, window = 16, 6
+    loss_ref, dU_ref, dG_ref = oracle_ibm_gradients(make, links, G, steps, window)
+    run = AdjointRun(make, links, steps=steps, window=window, checkpoint=5)
+    loss = run.forward(1.0, G)
+    dU, dG = run.backward()
+    assert loss == pytest.approx(loss_ref, rel=1e-12)
+    assert dU == pytest.approx(dU_ref, rel=1e-10)
+    fluid = p.fluid
+    np.testing.assert_allclose(dG[:, fluid], dG_ref[:, fluid], rtol=0, atol=1e-10 * np.abs(dG_ref).max())
+
+
+def test_immersed_body_adjoint_matches_central_finite_differences():
+    """float64 GPU runs, h = 1e-4 relative; agreement <= 1e-6 (the target is 1e-4)."""
+    make, links, p = ibm_channel(2, "float64")
+    rng = np.random.default_rng(5)
+    G = 1e-5 * rng.standard_normal((p.d, *p.shape)) * p.fluid
+    steps, window = 60, 20
+    run = AdjointRun(make, links, steps=steps, window=window, checkpoint=16)
+    run.forward(1.0, G)
+    dU, dG = run.backward()
+    h = 1e-4
+    fd_U = (run.forward(1.0 + h, G) - run.forward(1.0 - h, G)) / (2 * h)
+    assert abs(dU - fd_U) <= 1e-6 * abs(fd_U)
+    v = rng.standard_normal(G.shape) * p.fluid
+    eps = 1e-4 * np.abs(G).max()
+    fd_G = (run.forward(1.0, G + eps * v) - run.forward(1.0, G - eps * v)) / (2 * eps)
+    assert abs((dG * v).sum() - fd_G) <= 1e-6 * abs(fd_G)
+
+
+def test_float32_immersed_body_adjoint_is_close_to_float64():
+    make64, links, p = ibm_channel(3, "float64")
+    make32, _, _ = ibm_channel(3, "float32")
+    rng = np.random.default_rng(6)
+    G = 1e-5 * rng.standard_normal((p.d, *p.shape)) * p.fluid
+    out = []
+    for make in (make64, make32):
+        run = AdjointRun(make, links, steps=40, window=15, checkpoint=10)
+        run.forward(1.0, G)
+        out.append(run.backward())
+    (dU64, dG64), (dU32, dG32) = out
+    assert dU32 == pytest.approx(dU64, rel=1e-4)
+    assert np.abs(dG32 - dG64).max() <= 1e-4 * np.abs(dG64).max()
+
+
+def test_immersed_body_loss_needs_an_immersed_body():
+    make, links, p = channel_2d("float64")
+    run = AdjointRun(make, None, steps=4, window=2)
+    with pytest.raises(ValueError, match="immersed"):
+        run.forward(1.0, None)
