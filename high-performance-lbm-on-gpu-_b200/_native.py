@@ -114,6 +114,7 @@ _SIGNATURES = {
     "lbm_affine_reduce_static": [i32, vp, vp, vp, vp, vp, i64, i32, i32, vp, vp],
     "lbm_ibm_moments": [P(Grid), P(Physics), P(Ibm), vp, i32, vp],
     "lbm_ibm_iteration": [P(Grid), P(Ibm), i32, vp, vp, vp],
+    "lbm_ibm_force": [P(Grid), P(Physics), P(Ibm), vp, i32, i32, vp, vp],
     "lbm_ibm_body_force": [P(Grid), P(Ibm), i32, vp, vp],
     "lbm_ibm_adjoint_iteration": [P(Grid), P(Ibm), vp, vp, i32, C.c_double, vp, vp, vp],
     "lbm_ibm_adjoint_moments": [P(Grid), P(Ibm), vp, vp, vp],

@@ -126,7 +126,7 @@ class AdjointRun:
             "rho": torch.zeros(n, dtype=real, device=dev),
             "u_star": torch.zeros((d, n), dtype=real, device=dev),
             "marker_force": torch.zeros((tab.iterations, d, tab.n_markers), dtype=real, device=dev),
-            "force": [torch.zeros((d, n), dtype=real, device=dev) for _ in range(tab.iterations)],
+            "force": torch.zeros((tab.iterations, d, n), dtype=real, device=dev),
             "adj": [torch.zeros((d, n), dtype=real, device=dev) for _ in range(2)],
             "moments": torch.zeros((1 + d, n), dtype=torch.float64, device=dev),
         }
@@ -137,13 +137,10 @@ class AdjointRun:
         return st
 
     def _ibm_recompute(self, f, stream):
-        """The multi-direct passes of the step from state f, keeping every pass's node force."""
+        """The multi-direct passes of the step from state f (as the forward step), every pass's node force kept."""
         s, st = self.solver, self._ibm_adj
-        g = N.C.byref(s.grid)
-        N.call("lbm_ibm_moments", g, N.C.byref(s.physics), N.C.byref(st["struct"]), N.ptr(f), N.LAYOUT_PULL, stream)
-        for it, out in enumerate(st["force"]):
-            fin = st["force"][it - 1] if it else None
-            N.call("lbm_ibm_iteration", g, N.C.byref(st["struct"]), it, N.ptr(fin), N.ptr(out), stream)
+        N.call("lbm_ibm_force", N.C.byref(s.grid), N.C.byref(s.physics), N.C.byref(st["struct"]), N.ptr(f),
+               N.LAYOUT_PULL, st["force"].shape[0], N.ptr(st["force"]), stream)
 
     def _ibm_reverse(self, mu, body_scale, stream):
         """Passes in reverse from dL/d(node force) (written by the adjoint step), then add the moment

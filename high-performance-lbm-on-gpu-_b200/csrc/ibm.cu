@@ -19,12 +19,10 @@
 namespace lbm {
 
 template <class L, int ST>
-__global__ void ibm_moments_kernel(const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib,
-                                   const typename Storage<ST>::T* __restrict__ f, int layout)
+__device__ __forceinline__ void ibm_moments_node(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib,
+                                                 const typename Storage<ST>::T* __restrict__ f, int layout, int n)
 {
     using R = typename Storage<ST>::R;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= ib.n_nodes) return;
     const int64_t nd = ib.node[n];
     const int64_t row = nd / g.pitch;
     const int x = (int)(nd - row * g.pitch), y = (int)(row % g.ny), z = (int)(row / g.ny);
@@ -57,6 +55,96 @@ __global__ void ibm_moments_kernel(const lbm_grid_t g, const lbm_physics_t p, co
     us[n] = (jx + R(0.5) * R(p.force[0])) / rho;
     us[ib.n_nodes + n] = (jy + R(0.5) * R(p.force[1])) / rho;
     if (L::D == 3) us[2 * ib.n_nodes + n] = (jz + R(0.5) * R(p.force[2])) / rho;
+}
+
+template <class L, int ST>
+__global__ void ibm_moments_kernel(const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib,
+                                   const typename Storage<ST>::T* __restrict__ f, int layout)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < ib.n_nodes) ibm_moments_node<L, ST>(g, p, ib, f, layout, n);
+}
+
+// ---------------------------------------------------------------- one launch per step
+// Moments and every multi-direct pass of one step in a single block, for
+// bodies of up to IBM_FUSED_MAX stencil nodes and markers: phases separated
+// by __syncthreads instead of launches. Per pass the marker forces are formed
+// once per marker (threads over markers), then spread node-centric (threads
+// over nodes) -- the same operations, in the same order, as the per-pass
+// kernel, so both paths give the same bits. Buffers written inside the kernel
+// are read with plain loads (one block, one SM: its L1 sees its own stores).
+// Threads of the block: 512 in 3D, where a marker's 27-node stencil needs
+// more registers (no spills at 128 per thread).
+template <class L> constexpr int ibm_fused_threads() { return L::D == 2 ? 1024 : 512; }
+constexpr int IBM_FUSED_MAX = 4096;
+
+template <class L, int ST>
+__global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel(
+    const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib, const typename Storage<ST>::T* __restrict__ f,
+    int layout, int iterations, typename Storage<ST>::R* force)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    constexpr int S = D == 2 ? 9 : 27;
+    const int nn = ib.n_nodes, nm = ib.n_markers;
+    for (int n = threadIdx.x; n < nn; n += blockDim.x) ibm_moments_node<L, ST>(g, p, ib, f, layout, n);
+    __syncthreads();
+    const R* rho = (const R*)ib.rho;
+    const R* us = (const R*)ib.u_star;
+    const R* __restrict__ wgt = (const R*)ib.weight;
+    const R* __restrict__ area = (const R*)ib.area;
+    const R* __restrict__ invw = (const R*)ib.inv_weight;
+    for (int it = 0; it < iterations; ++it) {
+        const R* fin = it == 0 ? nullptr : force + (int64_t)(it - 1) * D * nn;
+        R* fout = force + (int64_t)it * D * nn;
+        R* mf = (R*)ib.marker_force + (int64_t)it * D * nm;
+        for (int l = threadIdx.x; l < nm; l += blockDim.x) {
+            const int* st = ib.stencil + (int64_t)l * S;
+            const R* wl = wgt + (int64_t)l * S;
+            int m[S];
+            R w[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                m[s] = st[s];
+                w[s] = wl[s];
+            }
+            R rho_l = R(0);
+            R U[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) U[a] = R(0);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const R rm = rho[m[s]];
+                rho_l += w[s] * rm;
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    R u = us[a * nn + m[s]];
+                    if (fin != nullptr) u += fin[a * nn + m[s]] / (R(2) * rm);
+                    U[a] += w[s] * u;
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a) mf[(int64_t)a * nm + l] = R(2) * rho_l * (R(0) - U[a]) * area[l];
+        }
+        __syncthreads();
+        for (int n = threadIdx.x; n < nn; n += blockDim.x) {
+            double acc[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) acc[a] = 0.0;
+            for (int q = ib.inv_start[n]; q < ib.inv_start[n + 1]; ++q) {
+                const int l = ib.inv_marker[q];
+                const R wn = invw[q];
+#pragma unroll
+                for (int a = 0; a < D; ++a) acc[a] += (double)(wn * mf[(int64_t)a * nm + l]);
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                const double base = fin != nullptr ? (double)fin[a * nn + n] : 0.0;
+                fout[a * nn + n] = (R)(base + acc[a]);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 template <class L, int ST>
@@ -266,6 +354,26 @@ int ibm_moments(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib
 }
 
 template <class L, int ST>
+int ibm_force(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, const void* f, int layout,
+              int iterations, void* force, cudaStream_t s)
+{
+    using R = typename Storage<ST>::R;
+    using T = typename Storage<ST>::T;
+    if (ib.n_nodes <= 0) return LBM_OK;
+    R* out = (R*)force;
+    if (ib.n_nodes <= IBM_FUSED_MAX && ib.n_markers <= IBM_FUSED_MAX) {
+        ibm_force_fused_kernel<L, ST><<<1, ibm_fused_threads<L>(), 0, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
+        return launch_status();
+    }
+    ibm_moments_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(g, p, ib, (const T*)f, layout);
+    const int64_t plane = (int64_t)L::D * ib.n_nodes;
+    for (int it = 0; it < iterations; ++it)
+        ibm_iteration_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(
+            ib, it, it == 0 ? nullptr : out + (it - 1) * plane, out + it * plane);
+    return launch_status();
+}
+
+template <class L, int ST>
 int ibm_iteration(const lbm_grid_t& g, const lbm_ibm_t& ib, int iteration, const void* fin, void* fout, cudaStream_t s)
 {
     using R = typename Storage<ST>::R;
@@ -302,6 +410,14 @@ extern "C" int lbm_ibm_moments(const lbm_grid_t* g, const lbm_physics_t* p, cons
     if (!ibm_ok(g, ib) || !p || !f) return LBM_ERR_INVALID;
     if (layout < LBM_LAYOUT_PULL || layout > LBM_LAYOUT_AA_EVEN) return LBM_ERR_INVALID;
     LBM_DISPATCH(g->lattice, g->storage, ibm_moments, *g, *p, *ib, f, layout, (cudaStream_t)stream);
+}
+
+extern "C" int lbm_ibm_force(const lbm_grid_t* g, const lbm_physics_t* p, const lbm_ibm_t* ib, const void* f,
+                             int32_t layout, int32_t iterations, void* force, lbm_stream_t stream)
+{
+    if (!ibm_ok(g, ib) || !p || !f || !force || iterations < 1) return LBM_ERR_INVALID;
+    if (layout < LBM_LAYOUT_PULL || layout > LBM_LAYOUT_AA_EVEN) return LBM_ERR_INVALID;
+    LBM_DISPATCH(g->lattice, g->storage, ibm_force, *g, *p, *ib, f, layout, iterations, force, (cudaStream_t)stream);
 }
 
 extern "C" int lbm_ibm_iteration(const lbm_grid_t* g, const lbm_ibm_t* ib, int32_t iteration, const void* force_in,

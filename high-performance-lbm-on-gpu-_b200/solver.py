@@ -541,10 +541,17 @@ class CudaSolver(Solver):
         return self._f
 
     # ------------------------------------------------------------------ stepping
-    def _step_launch(self, name, sp, *tail):
-        """One time step: a fused launch, or bulk + boundary kernels forked onto two streams."""
+    def _step_launch(self, name, sp, *tail, before_boundary=None):
+        """One time step: a fused launch, or bulk + boundary kernels forked onto two streams.
+
+        ``before_boundary(stream)`` (the immersed-boundary force of a pull step) runs first: on the side
+        stream ahead of the boundary kernel when the launch is split, so that it overlaps the bulk
+        kernel, which neither reads nor writes what it touches; else ahead of the step on this stream.
+        """
         g, ph = N.C.byref(self.grid), N.C.byref(self.physics)
         if self.launch_mode == "fused" or self._special.n_special == 0:
+            if before_boundary is not None:
+                before_boundary(self._stream())
             mode = N.LAUNCH_FUSED if (self._special.n_special and self.launch_mode == "fused") else N.LAUNCH_BULK
             self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[mode]), N.ptr(self._kind), *tail,
                          self._stream())
@@ -555,6 +562,8 @@ class CudaSolver(Solver):
         fork, join = torch.cuda.Event(), torch.cuda.Event()
         fork.record(main)
         side.wait_event(fork)
+        if before_boundary is not None:
+            before_boundary(side.cuda_stream)
         self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[N.LAUNCH_BOUNDARY]), N.ptr(self._kind), *tail,
                      side.cuda_stream)
         join.record(side)
@@ -570,10 +579,11 @@ class CudaSolver(Solver):
         return s
 
     def _launch_pull(self):
-        if self._ibm is not None:
-            self._ibm.run(self._f, N.LAYOUT_PULL)
+        # the immersed-boundary force reads f_src only and feeds only the boundary kernel
+        f = self._f
+        ibm = None if self._ibm is None else (lambda stream: self._ibm.run(f, N.LAYOUT_PULL, stream))
         sp = self._special_struct()
-        self._step_launch("lbm_step_pull", sp, N.ptr(self._f), N.ptr(self._f_next))
+        self._step_launch("lbm_step_pull", sp, N.ptr(self._f), N.ptr(self._f_next), before_boundary=ibm)
         self._f, self._f_next = self._f_next, self._f
 
     def _launch_aa(self, parity, layout):
@@ -757,8 +767,9 @@ class _IbmState:
             "u_star": torch.zeros((d, tables.n_nodes), dtype=real, device=dev),
             "marker_force": torch.zeros((tables.iterations, d, tables.n_markers), dtype=real, device=dev),
         }
-        self.force = [torch.zeros((d, tables.n_nodes), dtype=real, device=dev) for _ in range(2)]
-        self.final_force = self.force[(tables.iterations - 1) % 2]
+        # node force after every pass; the last pass's is the one the step adds
+        self.force = torch.zeros((tables.iterations, d, tables.n_nodes), dtype=real, device=dev)
+        self.final_force = self.force[tables.iterations - 1]
         self._body = torch.zeros(d, dtype=torch.float64, device=dev)
         g = self._t.get
         self.struct = N.Ibm(
@@ -767,13 +778,11 @@ class _IbmState:
             N.ptr(g("inv_weight")), N.ptr(g("rho")), N.ptr(g("u_star")), N.ptr(g("marker_force")),
         )
 
-    def run(self, f, layout: int) -> None:
+    def run(self, f, layout: int, stream=None) -> None:
+        """Node force of the step from state f (moments + every multi-direct pass, one call)."""
         s = self.solver
-        stream = s._stream()
-        N.call("lbm_ibm_moments", N.C.byref(s.grid), N.C.byref(s.physics), N.C.byref(self.struct), N.ptr(f), layout, stream)
-        for it in range(self.tables.iterations):
-            fin = None if it == 0 else self.force[(it - 1) % 2]
-            N.call("lbm_ibm_iteration", N.C.byref(s.grid), N.C.byref(self.struct), it, N.ptr(fin), N.ptr(self.force[it % 2]), stream)
+        N.call("lbm_ibm_force", N.C.byref(s.grid), N.C.byref(s.physics), N.C.byref(self.struct), N.ptr(f), layout,
+               self.tables.iterations, N.ptr(self.force), s._stream() if stream is None else stream)
 
     def body_force(self) -> np.ndarray:
         s = self.solver

@@ -263,6 +263,17 @@ int lbm_ibm_moments(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm
 int lbm_ibm_iteration(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iteration,
                       const void* force_in, void* force_out, lbm_stream_t stream);
 
+/* The immersed-boundary node force of one step in one call: moments of the
+ * state f (in layout) and `iterations` multi-direct passes -- replaces the
+ * array code of ImmersedForcing.force_field (src/lbm/ibm.py:189-214, run
+ * before every step by src/lbm/solver.py). force: real[iterations][d][n_nodes],
+ * pass j written to force[j] (the last pass is the node force the step adds);
+ * marker forces of every pass in ibm->marker_force as lbm_ibm_iteration.
+ * Bodies of up to 4096 stencil nodes and markers run as one one-block launch;
+ * larger ones as lbm_ibm_moments + one lbm_ibm_iteration launch per pass. */
+int lbm_ibm_force(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm_ibm_t* ibm, const void* f,
+                  int32_t layout, int32_t iterations, void* force, lbm_stream_t stream);
+
 /* Body force -sum_iterations sum_l F_l in float64 (out[d]). */
 int lbm_ibm_body_force(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iterations, double* out,
                        lbm_stream_t stream);
