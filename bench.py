@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched-cavities study (aggregate MLUPS against separate launches)")
+    ap.add_argument("--study", choices=("tgv", "cylinder", "batched", "adjoint", "precision"), default=None,
+                    help="run one configuration study alone and print its JSON (no duct line)")
+    ap.add_argument("--study-steps", type=int, default=None, help="steps of --study (default: the study's own)")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the Taylor-Green and cylinder configuration studies")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
@@ -203,8 +206,10 @@ def measured_peak():
 
 def step_kernel_name(args) -> str:
     """The kernel that carries the duct step (one launch per step)."""
-    if args.variant == "pull" and args.storage in ("float16", "bfloat16") and args.launch == "split":
-        return f"lbm_tma_pull_kernel<D3Q19, {args.storage}>"
+    if args.storage in ("float16", "bfloat16") and args.launch == "split":
+        if args.variant == "pull":
+            return f"lbm_tma_pull_kernel<D3Q19, {args.storage}>"
+        return f"lbm_tma_aa_kernel<D3Q19, {args.storage}, aa_odd + aa_even>"
     return f"lbm_bulk_kernel<D3Q19, {args.storage}, {args.variant}>"
 
 
@@ -270,7 +275,7 @@ def precision_study(lbm, torch, n: int, steps: int, variant: str):
     return out
 
 
-def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: int = 100):
+def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: int = 100, fd: bool = True):
     """Adjoint configuration: D3Q19 channel 128 x 64 x 64, Bouzidi sphere r = 8, Zou-He inlet U = 0.04,
     pressure outlet, tau = 0.6, loss = drag averaged over the last `window` of `steps` steps,
     gradients w.r.t. the inlet-speed scale U and a per-node Guo force field G ~ N(0, 1e-7^2).
@@ -319,6 +324,8 @@ def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: 
     fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
     out["float32"] = {"loss": loss, "dL_dU": dU, "forward_ms_per_step": round(fwd / steps, 5),
                       "backward_ms_per_step": round(bwd / steps, 5), "backward_over_forward": round(bwd / fwd, 3)}
+    if not fd:
+        return out
     make64, links64, p64 = case("float64")
     run = AdjointRun(make64, links64, steps=steps, window=window, checkpoint=checkpoint)
     run.forward(1.0, G)
@@ -607,6 +614,28 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_study(args):
+    """One configuration study on cuda:0 (for profiling one kernel family at a time)."""
+    import torch
+
+    import lbm_b200 as lbm
+
+    torch.cuda.set_device(0)
+    k = args.study_steps
+    if args.study == "tgv":
+        result = tgv_study(lbm, torch, **({"steps": k} if k else {}))
+    elif args.study == "cylinder":
+        result = cylinder_study(lbm, torch, **({"steps": k} if k else {}))
+    elif args.study == "batched":
+        result = batched_study(lbm, torch, **({"steps": k} if k else {}))
+    elif args.study == "adjoint":
+        kw = {"steps": k, "window": max(1, k // 4), "fd": False} if k else {}
+        result = adjoint_study(lbm, torch, **kw)
+    else:
+        result = precision_study(lbm, torch, args.n, k or args.precision_steps, args.variant)
+    print(json.dumps({"study": args.study, "result": result}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -614,6 +643,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.study is not None:
+        run_study(args)
         return
     if world > 1:
         import datetime

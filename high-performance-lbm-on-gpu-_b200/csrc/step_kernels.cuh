@@ -382,6 +382,129 @@ __global__ void __launch_bounds__(256) lbm_bulk_vec_kernel(const StepArgs a)
     VecPull<L, ST>::run(a, warp_x * 64, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
 
+// ---------------------------------------------------------------- vector AA
+// The in-place AA step for 16-bit storage with node pairs (x even, x + 1)
+// per thread, as VecPull: 4-byte loads and stores, two collisions, one
+// cvt.rs per direction for both results.
+//   * even (node-local): pair i read from slot i, written to slot opp(i) of
+//     the same pair -- no neighbour, so any warp without SOLID or SPECIAL
+//     nodes takes it (walls and faces do not matter here).
+//   * odd: read slot opp(i) of x - c_i (the VecPull gather: x shifts by
+//     warp shuffle, the node beyond the warp's range loaded by lane 0 or 31)
+//     and write slot i of x + c_i. For c_x != 0 the destination pairs
+//     straddle the source pairs: each lane rounds its own two results (its
+//     own random word, as the one-node path), then a shuffle hands the half
+//     that crosses to the neighbouring lane, which stores the assembled
+//     pair; the half leaving the warp's range is stored alone (2 bytes) by
+//     lane 0 or 31, and the slot whose source lies outside the range is left
+//     to the warp that owns that source. Every slot is written once. Taken
+//     by warps of interior nodes (periodic x faces included), rows off the y
+//     and z faces.
+// Other warps update their nodes one at a time (bulk_node). Same bits as the
+// one-node path.
+template <class L, int ST, int VAR>
+struct VecAA {
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    static constexpr int Q = L::Q;
+    static constexpr int V = 2;
+    static_assert(sizeof(T) == 2, "two 16-bit populations per word");
+    static_assert(VAR == LBM_AA_EVEN || VAR == LBM_AA_ODD, "AA halves only");
+
+    __device__ static __forceinline__ void run(const StepArgs& a, int x_base, int y, int z)
+    {
+        constexpr unsigned FULL = 0xffffffffu;
+        const int lane = threadIdx.x & 31;
+        const int64_t qs = a.qstride;
+        const int64_t py = a.pitch;
+        const int64_t pz = (int64_t)a.pitch * a.ny;
+        const int64_t row = (int64_t)z * pz + (int64_t)y * py;
+        const int x0 = x_base + V * lane;
+        const int64_t nd0 = row + x0;
+        const bool in_row = y < a.ny;
+        bool fast = in_row && x_base + 32 * V <= a.nx;
+        if (VAR == LBM_AA_ODD) fast = fast && y > 0 && y < a.ny - 1 && (L::D == 2 || (z > 0 && z < a.nz - 1));
+        if (fast) {
+            const uint32_t k2 = *reinterpret_cast<const unsigned short*>(a.kind + nd0);
+            fast = VAR == LBM_AA_EVEN ? (k2 & 0x0303u) == 0u : (k2 & ~0x0808u) == 0u;
+        }
+        if (!__all_sync(FULL, fast)) {
+            for (int j = 0; j < V; ++j) {
+                const int x = x_base + 32 * j + lane;
+                bulk_node<L, ST, VAR>(a, x, y, z, row + x, in_row && x < a.nx);
+            }
+            return;
+        }
+        // periodic x: the nodes just outside the warp's range
+        const int x_lo = x_base == 0 ? a.nx - 1 : x_base - 1;
+        const int x_hi = x_base + 32 * V == a.nx ? 0 : x_base + 32 * V;
+        T* f = static_cast<T*>(a.f_dst);  // in place: f_src == f_dst
+        R fa[Q], fb[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            uint32_t s;
+            if (VAR == LBM_AA_EVEN) {
+                s = *reinterpret_cast<const uint32_t*>(f + i * qs + nd0);
+            } else {
+                const int64_t src_row = row - (L::cy(i) * py + L::cz(i) * pz) + L::opp(i) * qs;
+                const uint32_t w = *reinterpret_cast<const uint32_t*>(f + src_row + x0);
+                s = w;
+                if (L::cx(i) > 0) {  // sources x - 1
+                    uint32_t pw = __shfl_up_sync(FULL, w, 1);
+                    if (lane == 0) pw = (uint32_t)*reinterpret_cast<const unsigned short*>(f + src_row + x_lo) << 16;
+                    s = __byte_perm(pw, w, 0x5432);
+                } else if (L::cx(i) < 0) {  // sources x + 1
+                    uint32_t nw = __shfl_down_sync(FULL, w, 1);
+                    if (lane == 31) nw = *reinterpret_cast<const unsigned short*>(f + src_row + x_hi);
+                    s = __byte_perm(w, nw, 0x5432);
+                }
+            }
+            fa[i] = S::decode_lo(s);
+            fb[i] = S::decode_hi(s);
+        }
+        const Relax<R>& rc = a.template relax<R>();
+        const R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
+        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        const uint32_t h = sr_pair_hash(sr_pair(a.nx, a.ny, x0, y, z), a.seed[a.parity]);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const uint32_t w = S::pack_sr(fa[i], fb[i], sr_word(h, i));  // (x0, x0 + 1) rounded
+            if (VAR == LBM_AA_EVEN) {
+                *reinterpret_cast<uint32_t*>(f + L::opp(i) * qs + nd0) = w;
+                continue;
+            }
+            T* dst_row = f + i * qs + row + (L::cy(i) * py + L::cz(i) * pz);
+            if (L::cx(i) == 0) {
+                *reinterpret_cast<uint32_t*>(dst_row + x0) = w;
+            } else if (L::cx(i) > 0) {  // x -> x + 1: pair (x0, x0 + 1) <- (lane - 1's odd node, own even node)
+                const uint32_t pw = __shfl_up_sync(FULL, w, 1);
+                if (lane == 0)
+                    *reinterpret_cast<unsigned short*>(dst_row + x0 + 1) = (unsigned short)(w & 0xffffu);
+                else
+                    *reinterpret_cast<uint32_t*>(dst_row + x0) = __byte_perm(pw, w, 0x5432);
+                if (lane == 31) *reinterpret_cast<unsigned short*>(dst_row + x_hi) = (unsigned short)(w >> 16);
+            } else {  // x -> x - 1: pair (x0, x0 + 1) <- (own odd node, lane + 1's even node)
+                const uint32_t nw = __shfl_down_sync(FULL, w, 1);
+                if (lane == 31)
+                    *reinterpret_cast<unsigned short*>(dst_row + x0) = (unsigned short)(w >> 16);
+                else
+                    *reinterpret_cast<uint32_t*>(dst_row + x0) = __byte_perm(w, nw, 0x5432);
+                if (lane == 0) *reinterpret_cast<unsigned short*>(dst_row + x_lo) = (unsigned short)(w & 0xffffu);
+            }
+        }
+    }
+};
+
+template <class L, int ST, int VAR>
+__global__ void __launch_bounds__(256) lbm_bulk_vec_aa_kernel(const StepArgs a)
+{
+    advance_seed(a);
+    const int warp_x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    VecAA<L, ST, VAR>::run(a, warp_x * 64, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
+}
+
 // Storage formats with the pair and TMA kernels (float32 and float64 keep
 // the one-node kernel: it is faster there).
 template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_BF16; }
@@ -405,9 +528,18 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
 }
 
 // Bulk-only launches: ptxas's default register target (no spills, high
-// occupancy) -- this kernel carries almost all of the traffic.
+// occupancy) -- this kernel carries almost all of the traffic. The odd AA
+// half (wrapped reads and wrapped writes on its general path) would take 74
+// registers in float32 arithmetic; four 256-thread blocks per SM cap it at
+// 64 without spills (32 resident warps instead of 24).
+template <int ST, int VAR>
+constexpr int bulk_min_blocks()
+{
+    return VAR == LBM_AA_ODD && sizeof(typename Storage<ST>::R) == 4 ? 4 : 0;
+}
+
 template <class L, int ST, int VAR>
-__global__ void __launch_bounds__(256) lbm_bulk_kernel(const StepArgs a)
+__global__ void __launch_bounds__(256, bulk_min_blocks<ST, VAR>()) lbm_bulk_kernel(const StepArgs a)
 {
     advance_seed(a);
     bulk_tile<L, ST, VAR>(a, blockIdx.z);
@@ -453,12 +585,22 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
         if (a.nz > 65535) return LBM_ERR_INVALID;
         if constexpr (VAR == LBM_PULL && has_vec<ST>()) {
             int status = LBM_OK;
-            if (launch_tma_pull<L, ST>(a, stream, &status)) return status;
+            if (launch_tma<L, ST, LBM_PULL>(a, stream, &status)) return status;
             // pairs need every row and direction plane to start on an even
             // node, and the launch's uniform-force constants
             if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
                 const unsigned gxv = (unsigned)((a.nx + 2 * tile_x - 1) / (2 * tile_x));
                 lbm_bulk_vec_kernel<L, ST><<<dim3(gxv, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+                return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+            }
+        }
+        if constexpr (VAR != LBM_PULL && has_vec<ST>()) {
+            int status = LBM_OK;
+            if (launch_tma<L, ST, VAR>(a, stream, &status)) return status;
+            // node pairs: every row and direction plane starts on an even node
+            if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
+                const unsigned gxv = (unsigned)((a.nx + 2 * tile_x - 1) / (2 * tile_x));
+                lbm_bulk_vec_aa_kernel<L, ST, VAR><<<dim3(gxv, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
                 return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
             }
         }

@@ -138,10 +138,128 @@ __device__ __forceinline__ void bounce(const StepArgs& a, typename Storage<ST>::
     }
 }
 
-template <class L, int ST>
-__global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_kernel(const __grid_constant__ CUtensorMap map,
-                                                                      const __grid_constant__ CUtensorMap kmap,
-                                                                      const StepArgs a, uint32_t* status)
+// One pair (x0, x0 + 1) of staged row r of an AA tile; st_row: direction 0's
+// staged row (direction i at st_row + i * plane), kind_row: the row's kinds.
+template <class L, int ST, int VAR>
+__device__ __forceinline__ void tma_aa_pair(const StepArgs& a, const typename Storage<ST>::T* st_row, int plane,
+                                            const unsigned char* kind_row, int x0, int y, int z,
+                                            const Relax<typename Storage<ST>::R>& rc, uint32_t t_seed)
+{
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    constexpr int Q = L::Q;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int64_t qs = a.qstride;
+    const int64_t nd0 = ((int64_t)z * ny + y) * a.pitch + x0;
+    const uint32_t k2 = *reinterpret_cast<const unsigned short*>(kind_row + x0);
+    const R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
+    R fa[Q], fb[Q];
+    if constexpr (VAR == LBM_AA_EVEN) {
+        const bool skip_a = (k2 & (KIND_SOLID | KIND_SPECIAL)) != 0u;
+        const bool skip_b = ((k2 >> 8) & (KIND_SOLID | KIND_SPECIAL)) != 0u;
+        if (y >= ny || (skip_a && skip_b)) return;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(st_row + i * plane + x0);
+            fa[i] = S::decode_lo(w);
+            fb[i] = S::decode_hi(w);
+        }
+        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        const uint32_t h = sr_pair_hash(sr_pair(nx, ny, x0, y, z), t_seed);
+        T* fd = static_cast<T*>(a.f_dst) + nd0;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const uint32_t w = S::pack_sr(fa[i], fb[i], sr_word(h, i));
+            T* d = fd + L::opp(i) * qs;
+            if (!skip_a && !skip_b) {
+                *reinterpret_cast<uint32_t*>(d) = w;
+            } else {
+                if (!skip_a) *reinterpret_cast<unsigned short*>(d) = (unsigned short)w;
+                if (!skip_b) *reinterpret_cast<unsigned short*>(d + 1) = (unsigned short)(w >> 16);
+            }
+        }
+    } else {
+        const bool staged = y >= 1 && y <= ny - 2 && (L::D == 2 || (z >= 1 && z <= nz - 2));
+        const bool ok = staged && (k2 & ~0x0808u) == 0u;  // both nodes interior (x faces allowed)
+        if (!__all_sync(FULL, ok)) {
+            for (int h = 0; h < 2; ++h) bulk_node<L, ST, LBM_AA_ODD>(a, x0 + h, y, z, nd0 + h, y < ny);
+            return;
+        }
+        const int lane = threadIdx.x & 31;
+        const int xm = x0 == 0 ? nx - 1 : x0 - 1;  // x0 - 1, wrapped
+        const int xp = x0 + 2 == nx ? 0 : x0 + 2;  // x0 + 2, wrapped
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const unsigned short* row = reinterpret_cast<const unsigned short*>(st_row + i * plane);
+            if (L::cx(i) == 0) {
+                const uint32_t w = *reinterpret_cast<const uint32_t*>(row + x0);
+                fa[i] = S::decode_lo(w);
+                fb[i] = S::decode_hi(w);
+            } else if (L::cx(i) > 0) {  // sources x0 - 1, x0
+                fa[i] = S::decode_lo(row[xm]);
+                fb[i] = S::decode_lo(row[x0]);
+            } else {  // sources x0 + 1, x0 + 2
+                fa[i] = S::decode_lo(row[x0 + 1]);
+                fb[i] = S::decode_lo(row[xp]);
+            }
+        }
+        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        const uint32_t h = sr_pair_hash(sr_pair(nx, ny, x0, y, z), t_seed);
+        // the warp's 64 nodes: [x_base, x_base + 64); the nodes beyond, wrapped
+        const int x_base = x0 - 2 * lane;
+        const int x_lo = x_base == 0 ? nx - 1 : x_base - 1;
+        const int x_hi = x_base + 64 == nx ? 0 : x_base + 64;
+        T* f = static_cast<T*>(a.f_dst);
+        const int64_t pz = (int64_t)a.pitch * ny;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const uint32_t w = S::pack_sr(fa[i], fb[i], sr_word(h, i));  // (x0, x0 + 1) rounded
+            T* dst_row = f + i * qs + ((int64_t)z * ny + y) * a.pitch + (L::cy(i) * a.pitch + L::cz(i) * pz);
+            if (L::cx(i) == 0) {
+                *reinterpret_cast<uint32_t*>(dst_row + x0) = w;
+            } else if (L::cx(i) > 0) {  // pair (x0, x0 + 1) <- (lane - 1's odd node, own even node)
+                const uint32_t pw = __shfl_up_sync(FULL, w, 1);
+                if (lane == 0)
+                    *reinterpret_cast<unsigned short*>(dst_row + x0 + 1) = (unsigned short)(w & 0xffffu);
+                else
+                    *reinterpret_cast<uint32_t*>(dst_row + x0) = __byte_perm(pw, w, 0x5432);
+                if (lane == 31) *reinterpret_cast<unsigned short*>(dst_row + x_hi) = (unsigned short)(w >> 16);
+            } else {  // pair (x0, x0 + 1) <- (own odd node, lane + 1's even node)
+                const uint32_t nw = __shfl_down_sync(FULL, w, 1);
+                if (lane == 31)
+                    *reinterpret_cast<unsigned short*>(dst_row + x0) = (unsigned short)(w >> 16);
+                else
+                    *reinterpret_cast<uint32_t*>(dst_row + x0) = __byte_perm(w, nw, 0x5432);
+                if (lane == 0) *reinterpret_cast<unsigned short*>(dst_row + x_lo) = (unsigned short)(w & 0xffffu);
+            }
+        }
+    }
+}
+
+// The staged step for one variant. PULL as described above. AA (in place,
+// one lattice; the caller requires nx >= 64, so a warp's 32 pairs are 64
+// consecutive nodes of one row):
+//   * AA_EVEN: the tile's own rows of slot i are staged; each pair is
+//     node-local (slot i in, slot opp(i) out), solid and SPECIAL nodes are
+//     skipped with 2-byte stores.
+//   * AA_ODD: rows y - c_y, z - c_z of slot opp(i) are staged; a warp of
+//     interior nodes (kinds 0 and EDGE, rows off the y and z faces) computes
+//     its pairs and pushes slot i to x + c_i: destination pairs straddle
+//     the source pairs along x, so each lane rounds its own two results and a
+//     shuffle hands the crossing half to the neighbouring lane; the half that
+//     leaves the warp's 64 nodes is stored alone by lane 0 or 31 (x wrapped
+//     in the row), and every slot is written once. Other warps update their
+//     nodes one by one (bulk_node).
+// In place is safe with loads in flight: slot (j, row) is read and written
+// only by the tile that owns its source node (the rows of a tile are whole
+// and x wraps inside them).
+template <class L, int ST, int VAR>
+__device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorMap& kmap, const StepArgs& a,
+                                         uint32_t* status)
 {
     using S = Storage<ST>;
     using T = typename S::T;
@@ -173,8 +291,13 @@ __global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_k
         unsigned char* dst = smem + s * stage_bytes;
         mbar_expect_tx(&bar[s], tx_bytes);
 #pragma unroll
-        for (int i = 0; i < Q; ++i)
-            tma_load_4d(dst + (size_t)i * plane * 2, &map, &bar[s], 0, y0 - L::cy(i), z - L::cz(i), i);
+        for (int i = 0; i < Q; ++i) {
+            if (VAR == LBM_AA_EVEN)
+                tma_load_4d(dst + (size_t)i * plane * 2, &map, &bar[s], 0, y0, z, i);
+            else
+                tma_load_4d(dst + (size_t)i * plane * 2, &map, &bar[s], 0, y0 - L::cy(i), z - L::cz(i),
+                            VAR == LBM_PULL ? i : L::opp(i));
+        }
         tma_load_3d(dst + pop_bytes, &kmap, &bar[s], 0, y0, z);
     };
 
@@ -239,6 +362,10 @@ __global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_k
             const int r = p >> log_half;
             const int x0 = 2 * (p - (r << log_half));
             const int y = y0 + r;
+            if constexpr (VAR != LBM_PULL) {
+                tma_aa_pair<L, ST, VAR>(a, st + r * nx, plane, kinds + r * nx, x0, y, z, rc, t_seed);
+                continue;
+            }
             // A fluid node takes the staged path when its source rows exist
             // (y, z inside the box faces); solid and SPECIAL nodes are left
             // alone (the boundary warps update the latter).
@@ -302,6 +429,22 @@ __global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_k
     }
 }
 
+template <class L, int ST>
+__global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_kernel(const __grid_constant__ CUtensorMap map,
+                                                                      const __grid_constant__ CUtensorMap kmap,
+                                                                      const StepArgs a, uint32_t* status)
+{
+    tma_step<L, ST, LBM_PULL>(map, kmap, a, status);
+}
+
+template <class L, int ST, int VAR>
+__global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_aa_kernel(const __grid_constant__ CUtensorMap map,
+                                                                    const __grid_constant__ CUtensorMap kmap,
+                                                                    const StepArgs a, uint32_t* status)
+{
+    tma_step<L, ST, VAR>(map, kmap, a, status);
+}
+
 // Driver entry point for tensor-map encoding (no link-time dependency on
 // the driver library).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -323,14 +466,26 @@ inline EncodeTiledFn encode_tiled_fn()
     return fn;
 }
 
-// Launch the TMA pull step if the grid qualifies; returns false (nothing
-// launched) when it does not, so the caller can take another kernel.
-template <class L, int ST>
-bool launch_tma_pull(const StepArgs& a, cudaStream_t stream, int* status_out)
+template <class L, int ST, int VAR>
+constexpr auto tma_kernel()
+{
+    if constexpr (VAR == LBM_PULL)
+        return lbm_tma_pull_kernel<L, ST>;
+    else
+        return lbm_tma_aa_kernel<L, ST, VAR>;
+}
+
+// Launch the TMA-staged step (pull, or one AA half in place) if the grid
+// qualifies; returns false (nothing launched) when it does not, so the
+// caller can take another kernel.
+template <class L, int ST, int VAR>
+bool launch_tma(const StepArgs& a, cudaStream_t stream, int* status_out)
 {
     *status_out = LBM_OK;
-    // whole rows of a power-of-two width in one box; rows of 16-byte multiples
-    if (a.nx < 16 || a.nx > 256 || (a.nx & (a.nx - 1)) != 0 || a.pitch % 16 != 0) return false;
+    // whole rows of a power-of-two width in one box; rows of 16-byte multiples;
+    // AA: a warp's 32 pairs within one row
+    const int nx_min = VAR == LBM_PULL ? 16 : 64;
+    if (a.nx < nx_min || a.nx > 256 || (a.nx & (a.nx - 1)) != 0 || a.pitch % 16 != 0) return false;
     if (reinterpret_cast<uintptr_t>(a.kind) % 16 != 0) return false;
     if (a.force_field != nullptr || !a.guo_const || a.seed == nullptr) return false;
     if (reinterpret_cast<uintptr_t>(a.f_src) % 16 != 0 || reinterpret_cast<uintptr_t>(a.f_dst) % 4 != 0) return false;
@@ -361,7 +516,7 @@ bool launch_tma_pull(const StepArgs& a, cudaStream_t stream, int* status_out)
     }
     static bool configured[64] = {};  // per device: the shared-memory opt-in of this kernel
     if (!configured[device]) {
-        if (cudaFuncSetAttribute(lbm_tma_pull_kernel<L, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(tma_kernel<L, ST, VAR>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(TMA_STAGES * tma_stage_bytes<L>(256) + 8 * TMA_STAGES)) != cudaSuccess) {
             cudaGetLastError();
             return false;
@@ -369,7 +524,7 @@ bool launch_tma_pull(const StepArgs& a, cudaStream_t stream, int* status_out)
         configured[device] = true;
     }
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_tma_pull_kernel<L, ST>, TMA_THREADS, smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tma_kernel<L, ST, VAR>(), TMA_THREADS, smem) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -378,7 +533,7 @@ bool launch_tma_pull(const StepArgs& a, cudaStream_t stream, int* status_out)
     const int64_t tiles = (int64_t)a.nz * ((a.ny + TMA_ROWS - 1) / TMA_ROWS);
     if (tiles > 0x7fffffff) return false;
     const int64_t grid = tiles < (int64_t)sms * per_sm ? tiles : (int64_t)sms * per_sm;
-    lbm_tma_pull_kernel<L, ST><<<(unsigned)grid, TMA_THREADS, smem, stream>>>(map, kmap, a, a.seed + 2);
+    tma_kernel<L, ST, VAR>()<<<(unsigned)grid, TMA_THREADS, smem, stream>>>(map, kmap, a, a.seed + 2);
     *status_out = cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
     return true;
 }
