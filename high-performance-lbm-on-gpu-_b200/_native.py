@@ -15,6 +15,7 @@ ABI_VERSION = 3
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
+DENSE_TERMS = 32
 LBM_D2Q9, LBM_D3Q19 = 0, 1
 LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
 LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
@@ -55,6 +56,7 @@ class Special(C.Structure):
         ("export_mask", vp), ("export_first", vp), ("n_rules", i32), ("n_terms", i32), ("term_start", vp),
         ("rule_const", vp), ("term_dir", vp), ("term_node", vp), ("term_export", vp), ("term_coeff", vp),
         ("local_force", vp), ("n_local", i32), ("n_export", i32), ("export_in", vp), ("export_out", vp),
+        ("ut_start", vp), ("ut_slot", vp), ("ut_export", vp), ("rule_row", vp), ("rule_dense", vp),
     ]
 
 
@@ -73,7 +75,7 @@ class Ibm(C.Structure):
 class Adjoint(C.Structure):
     _fields_ = [
         ("gather_start", vp), ("gather_dir", vp), ("gather_slot", vp), ("gather_coeff", vp), ("rule_dconst", vp),
-        ("term_dcoeff", vp), ("rule_du", vp), ("force_grad", vp), ("local_force_grad", vp),
+        ("term_dcoeff", vp), ("rule_du", vp), ("force_grad", vp), ("local_force_grad", vp), ("rule_ddense", vp),
     ]
 
 

@@ -240,6 +240,19 @@ class AdjointRun:
             self._adj_t["rule_dconst"] = torch.from_numpy(dconst).to(dev, s.t_real)
             self._adj_t["term_dcoeff"] = torch.from_numpy(dcoeff).to(dev, s.t_real)
             self._rule_du = torch.zeros(s._special.n_rules, dtype=torch.float64, device=dev)
+            if getattr(s, "_dense_pos", None) is not None:
+                ddense = np.zeros(t["rule_dense"].numel())
+                np.add.at(ddense, s._dense_pos, dcoeff)
+                self._adj_t["rule_ddense"] = torch.from_numpy(ddense).to(dev, s.t_real)
+        # dense rule form on the adjoint list: the forward nodes keep their distinct-term ranges (the
+        # lists are both sorted by node, so the ranges stay in order); the added nodes have none
+        if "ut_start" in t and base_nodes.size:
+            fwd_start = t["ut_start"].cpu().numpy().astype(np.int64)
+            before = np.searchsorted(base_nodes, nodes, side="left")  # forward nodes before each adjoint node
+            adj_start = np.zeros(ns + 1, dtype=np.int64)
+            adj_start[:-1] = fwd_start[before]
+            adj_start[-1] = fwd_start[-1]
+            self._adj_t["ut_start"] = torch.from_numpy(adj_start.astype(np.int32)).to(dev)
         self._force_grad = torch.zeros((lat.d, qs), dtype=s.t_real, device=dev)
 
     def _special_struct(self):
@@ -254,6 +267,9 @@ class AdjointRun:
             N.ptr(f.tensors.get("term_start")), N.ptr(f.tensors.get("rule_const")), N.ptr(f.tensors.get("term_dir")),
             N.ptr(f.tensors.get("term_node")), None, N.ptr(f.tensors.get("term_coeff")), N.ptr(local),
             f.n_local if st is not None else 0, 0, None, None,
+            N.ptr(g("ut_start")), N.ptr(f.tensors.get("ut_slot") if "ut_start" in t else None), None,
+            N.ptr(f.tensors.get("rule_row") if "ut_start" in t else None),
+            N.ptr(f.tensors.get("rule_dense") if "ut_start" in t else None),
         )
 
     def _adj_struct(self):
@@ -261,7 +277,8 @@ class AdjointRun:
         st = self._ibm_adj
         return N.Adjoint(N.ptr(t["gather_start"]), N.ptr(t["gather_dir"]), N.ptr(t["gather_slot"]),
                          N.ptr(t["gather_coeff"]), N.ptr(t.get("rule_dconst")), N.ptr(t.get("term_dcoeff")),
-                         N.ptr(self._rule_du), N.ptr(self._force_grad), N.ptr(st["adj"][0] if st is not None else None))
+                         N.ptr(self._rule_du), N.ptr(self._force_grad), N.ptr(st["adj"][0] if st is not None else None),
+                         N.ptr(t.get("rule_ddense")))
 
     # ------------------------------------------------------------------ forward
     def _probe_value(self, out_slot):

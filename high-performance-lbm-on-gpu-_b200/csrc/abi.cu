@@ -31,6 +31,10 @@ static bool special_valid(const lbm_special_t* sp, bool aa)
         if (!sp->term_start || !sp->rule_const || !sp->term_coeff) return false;
         if (aa ? !sp->term_export : (!sp->term_dir || !sp->term_node)) return false;
         if (aa && (!sp->export_in || sp->n_export <= 0)) return false;
+        if (sp->ut_start) {  // dense form
+            if (aa ? !sp->ut_export : !sp->ut_slot) return false;
+            if (!sp->rule_row || !sp->rule_dense || reinterpret_cast<uintptr_t>(sp->rule_dense) % 16 != 0) return false;
+        }
     }
     if (aa && sp->n_export > 0 && (!sp->export_mask || !sp->export_first || !sp->export_out)) return false;
     if (sp->n_local > 0 && !sp->local_force) return false;

@@ -211,6 +211,61 @@ struct AdjointKernel {
         }
     }
 
+    // The node's rules in the dense form: distinct term values loaded once,
+    // then per rule its value (coefficient row) and, with a U-derivative, the
+    // derivative row in float64 -- as rule_value_du, in two memory round trips
+    // for all the node's rules.
+    __device__ static __forceinline__ void dense_rules_du(const AdjArgs& A, int64_t s_idx, uint32_t rmask, int rfirst,
+                                                          bool with_du, R (&s)[Q], double (&dv)[Q])
+    {
+        constexpr int UM = LBM_DENSE_TERMS;
+        const StepArgs& a = A.a;
+        const lbm_special_t& sp = a.sp;
+        const int u0 = sp.ut_start[s_idx];
+        const int n = sp.ut_start[s_idx + 1] - u0;
+        const T* __restrict__ f = static_cast<const T*>(a.f_src);
+        int64_t slot[UM];
+        R v[UM];
+#pragma unroll
+        for (int u = 0; u < UM; ++u) slot[u] = u < n ? sp.ut_slot[u0 + u] : -1;
+#pragma unroll
+        for (int u = 0; u < UM; ++u) v[u] = slot[u] >= 0 ? S::load(f + slot[u]) : R(0);
+        const R* __restrict__ dense = static_cast<const R*>(sp.rule_dense);
+        const R* __restrict__ ddense = static_cast<const R*>(A.adj.rule_ddense);
+        const R* __restrict__ rconst = static_cast<const R*>(sp.rule_const);
+        const R* __restrict__ dconst = static_cast<const R*>(A.adj.rule_dconst);
+        uint32_t m = rmask;
+        int r = rfirst;
+        while (m) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1u;
+            const int row = sp.rule_row[r];
+            R acc = rconst[r];
+            double d = with_du ? (double)dconst[r] : 0.0;
+#pragma unroll
+            for (int u = 0; u < UM; u += 4) {
+                if (u < n) {
+                    R c[4];
+                    load4(dense + row + u, c);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) acc = v_fma(c[k], v[u + k], acc);
+                    if (with_du) {
+                        load4(ddense + row + u, c);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) d += (double)c[k] * (double)v[u + k];
+                    }
+                }
+            }
+            ++r;
+#pragma unroll
+            for (int j = 0; j < Q; ++j)
+                if (j == i) {
+                    s[j] = acc;
+                    dv[j] = d;
+                }
+        }
+    }
+
     // Any fluid node that is not interior: bounce-back and wrap; for nodes of
     // the adjoint list (s_idx >= 0) also rules, rule-term and loss gathers.
     // acc: this thread's column of a shared [Q][BOUNDARY_THREADS] array
@@ -223,6 +278,39 @@ struct AdjointKernel {
         const int x = (int)(nd - row * a.pitch), y = (int)(row % a.ny), z = (int)(row / a.ny);
         const int64_t qs = a.qstride;
         const uint32_t bb = a.nbr[nd];
+        // Rule-term and loss gathers into lambda, first (nothing else is live
+        // yet, so a batch can be wide): accumulated per direction in shared
+        // memory (a runtime direction index; in registers it would be a select
+        // over all Q directions per entry), added to lambda before the VJP.
+        // Entries thirty-two at a time: metadata, then the mu values.
+        if (s_idx >= 0) {
+            constexpr int BT = BOUNDARY_THREADS;
+#pragma unroll
+            for (int j = 0; j < Q; ++j) acc[j * BT] = R(0);
+            constexpr int B = 32;
+            const R* gc = static_cast<const R*>(A.adj.gather_coeff);
+            const R scale = R(A.loss_scale);
+            const R* mg = static_cast<const R*>(A.mu_next);
+            const int e1 = A.adj.gather_start[s_idx + 1];
+            for (int e0 = A.adj.gather_start[s_idx]; e0 < e1; e0 += B) {
+                int64_t slot[B];
+                int dir[B];
+                R c[B], val[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const bool in = e0 + k < e1;
+                    slot[k] = in ? A.adj.gather_slot[e0 + k] : -1;
+                    dir[k] = in ? A.adj.gather_dir[e0 + k] : 0;
+                    c[k] = in ? gc[e0 + k] : R(0);
+                }
+#pragma unroll
+                for (int k = 0; k < B; ++k) val[k] = (slot[k] >= 0 && mg != nullptr) ? mg[slot[k]] : R(0);
+#pragma unroll
+                for (int k = 0; k < B; ++k)
+                    if (e0 + k < e1) acc[dir[k] * BT] += slot[k] >= 0 ? c[k] * val[k] : c[k] * scale;
+            }
+        }
+
         const uint32_t rmask = s_idx >= 0 ? sp.rule_mask[s_idx] : 0u;
         const int rfirst = s_idx >= 0 ? sp.rule_first[s_idx] : 0;
         const int xm = wrap(x - 1, a.nx), xp = wrap(x + 1, a.nx);
@@ -262,7 +350,9 @@ struct AdjointKernel {
         double dv[Q];
 #pragma unroll
         for (int j = 0; j < Q; ++j) dv[j] = 0.0;
-        {
+        if (rmask && sp.ut_start != nullptr && (!with_du || A.adj.rule_ddense != nullptr)) {
+            dense_rules_du(A, s_idx, rmask, rfirst, with_du, s, dv);
+        } else {
             uint32_t m = rmask;
             int r = rfirst;
             while (m) {
@@ -283,37 +373,9 @@ struct AdjointKernel {
                     }
             }
         }
-        // rule-term and loss gathers into lambda, accumulated per direction in
-        // shared memory (a runtime direction index; in registers it would be
-        // a select over all Q directions per entry), then added to lambda
         if (s_idx >= 0) {
-            constexpr int BT = BOUNDARY_THREADS;
 #pragma unroll
-            for (int j = 0; j < Q; ++j) acc[j * BT] = R(0);
-            // entries sixteen at a time: metadata, then the mu values
-            constexpr int B = 16;
-            const R* gc = static_cast<const R*>(A.adj.gather_coeff);
-            const R scale = R(A.loss_scale);
-            const int e1 = A.adj.gather_start[s_idx + 1];
-            for (int e0 = A.adj.gather_start[s_idx]; e0 < e1; e0 += B) {
-                int64_t slot[B];
-                int dir[B];
-                R c[B], val[B];
-#pragma unroll
-                for (int k = 0; k < B; ++k) {
-                    const bool in = e0 + k < e1;
-                    slot[k] = in ? A.adj.gather_slot[e0 + k] : -1;
-                    dir[k] = in ? A.adj.gather_dir[e0 + k] : 0;
-                    c[k] = in ? gc[e0 + k] : R(0);
-                }
-#pragma unroll
-                for (int k = 0; k < B; ++k) val[k] = (slot[k] >= 0 && mn != nullptr) ? mn[slot[k]] : R(0);
-#pragma unroll
-                for (int k = 0; k < B; ++k)
-                    if (e0 + k < e1) acc[dir[k] * BT] += slot[k] >= 0 ? c[k] * val[k] : c[k] * scale;
-            }
-#pragma unroll
-            for (int j = 0; j < Q; ++j) lam[j] += acc[j * BT];
+            for (int j = 0; j < Q; ++j) lam[j] += acc[j * BOUNDARY_THREADS];
         }
         finish(A, nd, s, lam, s_idx);
         // d rule value / dU, weighted by mu of the ruled direction

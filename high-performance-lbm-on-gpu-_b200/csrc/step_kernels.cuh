@@ -34,6 +34,25 @@
 
 namespace lbm {
 
+// Four consecutive reals from a 16-byte aligned address (two loads for double).
+__device__ __forceinline__ void load4(const float* p, float (&c)[4])
+{
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    c[0] = q.x;
+    c[1] = q.y;
+    c[2] = q.z;
+    c[3] = q.w;
+}
+__device__ __forceinline__ void load4(const double* p, double (&c)[4])
+{
+    const double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 q1 = __ldg(reinterpret_cast<const double2*>(p + 2));
+    c[0] = q0.x;
+    c[1] = q0.y;
+    c[2] = q1.x;
+    c[3] = q1.y;
+}
+
 template <class L, int ST, int VAR>
 struct StepKernel {
     using S = Storage<ST>;
@@ -89,6 +108,57 @@ struct StepKernel {
             }
         }
         return v;
+    }
+
+    // The node's rules in the dense form (lbm_special_t.ut_start): its distinct
+    // term populations are loaded once, all in one batch, then each rule is a
+    // dot product with its coefficient row, read four at a time. Two memory
+    // round trips for all the node's rules.
+    __device__ static __forceinline__ void dense_rules(const StepArgs& a, int64_t s, uint32_t rmask, int rfirst,
+                                                       R (&f)[Q])
+    {
+        constexpr int UM = LBM_DENSE_TERMS;
+        const lbm_special_t& sp = a.sp;
+        const int u0 = sp.ut_start[s];
+        const int n = sp.ut_start[s + 1] - u0;
+        R v[UM];
+        if (VAR == LBM_PULL) {
+            const T* __restrict__ fs = static_cast<const T*>(a.f_src);
+            int64_t slot[UM];
+#pragma unroll
+            for (int u = 0; u < UM; ++u) slot[u] = u < n ? sp.ut_slot[u0 + u] : -1;
+#pragma unroll
+            for (int u = 0; u < UM; ++u) v[u] = slot[u] >= 0 ? S::load(fs + slot[u]) : R(0);
+        } else {
+            const R* __restrict__ ex = static_cast<const R*>(sp.export_in);
+            int e[UM];
+#pragma unroll
+            for (int u = 0; u < UM; ++u) e[u] = u < n ? sp.ut_export[u0 + u] : -1;
+#pragma unroll
+            for (int u = 0; u < UM; ++u) v[u] = e[u] >= 0 ? ex[e[u]] : R(0);
+        }
+        const R* __restrict__ dense = static_cast<const R*>(sp.rule_dense);
+        const R* __restrict__ rconst = static_cast<const R*>(sp.rule_const);
+        uint32_t m = rmask;
+        int r = rfirst;
+        while (m) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1u;
+            const R* row = dense + sp.rule_row[r];
+            R acc = rconst[r++];
+#pragma unroll
+            for (int u = 0; u < UM; u += 4) {
+                if (u < n) {
+                    R c[4];
+                    load4(row + u, c);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) acc = v_fma(c[k], v[u + k], acc);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < Q; ++j)
+                if (j == i) f[j] = acc;
+        }
     }
 
     // Interior fluid node (kind 0: no solid neighbour, not on a face of the
@@ -181,16 +251,20 @@ struct StepKernel {
         // ---- link rules replace the bounce-back value of their links. One
         // loop over the set bits keeps a single copy of the term loop; the
         // unrolled select writes the value without indexing f[] at run time.
-        if (SPECIAL) {
-            uint32_t m = rmask;
-            int r = rfirst;
-            while (m) {
-                const int i = __ffs(m) - 1;
-                m &= m - 1u;
-                const R v = rule_value(a, r++);
+        if (SPECIAL && rmask) {
+            if (a.sp.ut_start != nullptr) {
+                dense_rules(a, s, rmask, rfirst, f);
+            } else {
+                uint32_t m = rmask;
+                int r = rfirst;
+                while (m) {
+                    const int i = __ffs(m) - 1;
+                    m &= m - 1u;
+                    const R v = rule_value(a, r++);
 #pragma unroll
-                for (int j = 0; j < Q; ++j)
-                    if (j == i) f[j] = v;
+                    for (int j = 0; j < Q; ++j)
+                        if (j == i) f[j] = v;
+                }
             }
         }
 

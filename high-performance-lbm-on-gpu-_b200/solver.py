@@ -353,6 +353,7 @@ class CudaSolver(Solver):
             t["term_dir"] = torch.from_numpy(term_dir.astype(np.int32)).to(self.device)
             t["term_node"] = torch.from_numpy(self._pitched(term_node)).to(self.device)
             t["term_coeff"] = torch.from_numpy(term_coeff).to(self.device, self.t_real)
+            term_slot = term_dir * self.qstride + self._pitched(term_node)
         ibm_nodes = self._pitched(self._ibm.tables.nodes) if self._ibm is not None else np.zeros(0, dtype=np.int64)
         export_nodes = export_dirs = np.zeros(0, dtype=np.int64)
         if self.variant == "aa" and n_rules:
@@ -363,6 +364,7 @@ class CudaSolver(Solver):
             n_export = ukeys.size
             export_nodes, export_dirs = ukeys // 32, ukeys % 32
             t["term_export"] = torch.from_numpy(term_export.astype(np.int32)).to(self.device)
+            term_slot = term_export.astype(np.int64)  # the AA rules read the export buffer
             t["export_a"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
             t["export_b"] = torch.zeros(n_export, dtype=self.t_real, device=self.device)
 
@@ -395,6 +397,8 @@ class CudaSolver(Solver):
             pos = np.searchsorted(nodes, export_nodes)
             np.bitwise_or.at(export_mask, pos, (np.uint32(1) << export_dirs.astype(np.uint32)))
             export_first = np.searchsorted(export_nodes, nodes, side="left").astype(np.int32)
+        if n_rules:
+            self._dense_rules(t, nodes, rule_nodes, start, term_slot, term_coeff)
         t["node"] = marked_t
         t["rule_mask"] = torch.from_numpy(rule_mask.view(np.int32)).to(self.device)
         t["rule_first"] = torch.from_numpy(rule_first).to(self.device)
@@ -402,6 +406,37 @@ class CudaSolver(Solver):
         t["export_mask"] = torch.from_numpy(export_mask.view(np.int32)).to(self.device)
         t["export_first"] = torch.from_numpy(export_first).to(self.device)
         return _SpecialTables(t, ns, n_rules, n_terms, n_export, int(ibm_nodes.size))
+
+    def _dense_rules(self, t, nodes, rule_nodes, start, term_slot, term_coeff) -> None:
+        """Dense form of the rules (``lbm_special_t.ut_start``): per special node its rules' distinct terms,
+        per rule a coefficient row over them (rows padded to 4, zeros). Left out (term-by-term evaluation)
+        when a node's rules read more than ``DENSE_TERMS`` distinct populations."""
+        torch = self.torch
+        counts = np.diff(start)
+        n_rules = counts.size
+        rule_of_term = np.repeat(np.arange(n_rules), counts)
+        s_of_rule = np.searchsorted(nodes, rule_nodes)
+        s_of_term = s_of_rule[rule_of_term]
+        pairs, inverse = np.unique(np.stack([s_of_term, term_slot], axis=1), axis=0, return_inverse=True)
+        inverse = inverse.reshape(-1)
+        ut_start = np.searchsorted(pairs[:, 0], np.arange(nodes.size + 1))
+        n_distinct = np.diff(ut_start)
+        self._dense_pos = None
+        if n_distinct.max(initial=0) > N.DENSE_TERMS:
+            return
+        local = inverse - ut_start[s_of_term]
+        row_len = (n_distinct[s_of_rule] + 3) // 4 * 4
+        rule_row = np.zeros(n_rules, dtype=np.int64)
+        np.cumsum(row_len[:-1], out=rule_row[1:])
+        dense = np.zeros(max(int(row_len.sum()), 4))
+        self._dense_pos = rule_row[rule_of_term] + local  # dense position of every live term
+        np.add.at(dense, self._dense_pos, term_coeff)
+        dev = self.device
+        t["ut_start"] = torch.from_numpy(ut_start.astype(np.int32)).to(dev)
+        key = "ut_export" if self.variant == "aa" else "ut_slot"
+        t[key] = torch.from_numpy(pairs[:, 1].astype(np.int32 if self.variant == "aa" else np.int64)).to(dev)
+        t["rule_row"] = torch.from_numpy(rule_row.astype(np.int32)).to(dev)
+        t["rule_dense"] = torch.from_numpy(dense).to(dev, self.t_real)
 
     def _special_struct(self, export_in=None, export_out=None) -> N.Special:
         s = self._special
@@ -413,6 +448,8 @@ class CudaSolver(Solver):
             N.ptr(g("export_mask")), N.ptr(g("export_first")), s.n_rules, s.n_terms, N.ptr(g("term_start")),
             N.ptr(g("rule_const")), N.ptr(g("term_dir")), N.ptr(g("term_node")), N.ptr(g("term_export")),
             N.ptr(g("term_coeff")), N.ptr(local), s.n_local, s.n_export, N.ptr(export_in), N.ptr(export_out),
+            N.ptr(g("ut_start")), N.ptr(g("ut_slot")), N.ptr(g("ut_export")), N.ptr(g("rule_row")),
+            N.ptr(g("rule_dense")),
         )
 
     # ------------------------------------------------------------------ state

@@ -99,7 +99,21 @@ typedef struct lbm_special {
     int32_t n_export;
     const void* export_in;        /* AA: real[n_export] written by the previous launch */
     void* export_out;             /* AA: real[n_export] read by the next launch */
+    /* Optional dense form of the same rules (ut_start NULL: term by term).
+     * The rules of special node s read the distinct populations
+     * u in [ut_start[s], ut_start[s+1]) -- at most LBM_DENSE_TERMS -- and rule r
+     * of that node is  const[r] + sum_u rule_dense[rule_row[r] + u - ut_start[s]] * value(u),
+     * so each distinct population is loaded once for all the node's rules
+     * (a Zou-He node's five rules share its fourteen known populations). */
+    const int32_t* ut_start;      /* n_special + 1 */
+    const int64_t* ut_slot;       /* pull: slot (dir * qstride + pitched node) of each distinct term */
+    const int32_t* ut_export;     /* AA: export index of each distinct term */
+    const int32_t* rule_row;      /* n_rules: start of rule r's row, a multiple of 4 */
+    const void* rule_dense;       /* real, 16-byte aligned; rows zero-padded to multiples of 4 */
 } lbm_special_t;
+
+/* Distinct populations a special node's rules may read in the dense form. */
+#define LBM_DENSE_TERMS 32
 
 /* How a step is launched. The bulk grid covers every fluid node that is not
  * SPECIAL with blocks of tile_x * tile_y threads, one node each, over
@@ -321,6 +335,8 @@ typedef struct lbm_adjoint {
     void* local_force_grad;        /* real[d][n_local]: dL/dF at each special node with a force slot
                                       (sp->force_slot >= 0, the immersed-boundary stencil nodes, whose
                                       collision adds sp->local_force), written by every step, or NULL */
+    const void* rule_ddense;       /* real: d coeff / dU in the layout of sp->rule_dense (with sp->ut_start
+                                      set and rule_du wanted), or NULL: rules are evaluated term by term */
 } lbm_adjoint_t;
 
 /* One backward step of the two-lattice pull scheme, fused:
