@@ -601,15 +601,19 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
     StepKernel<L, ST, VAR>::template node<true>(a, x, y, z, nd, a.nbr[nd], s);
 }
 
-// Bulk-only launches: ptxas's default register target (no spills, high
-// occupancy) -- this kernel carries almost all of the traffic. The odd AA
-// half (wrapped reads and wrapped writes on its general path) would take 74
-// registers in float32 arithmetic; four 256-thread blocks per SM cap it at
-// 64 without spills (32 resident warps instead of 24).
+// Bulk-only launches -- this kernel carries almost all of the traffic, so
+// its register count sets the resident warps. ptxas's default target is
+// kept except where a bound does better without spills: the odd AA half
+// (wrapped reads and wrapped writes on its general path) would take 74
+// registers in float32 arithmetic, four 256-thread blocks per SM cap it at
+// 64 (32 resident warps instead of 24); the float32 pull would take 54, five
+// blocks cap it at 48 (40 warps instead of 36: 38.7 against 37.8 GLUPS).
 template <int ST, int VAR>
 constexpr int bulk_min_blocks()
 {
-    return VAR == LBM_AA_ODD && sizeof(typename Storage<ST>::R) == 4 ? 4 : 0;
+    if (VAR == LBM_AA_ODD && sizeof(typename Storage<ST>::R) == 4) return 4;
+    if (VAR == LBM_PULL && ST == LBM_F32) return 5;
+    return 0;
 }
 
 template <class L, int ST, int VAR>
