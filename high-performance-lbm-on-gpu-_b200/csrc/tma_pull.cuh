@@ -269,7 +269,7 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
     static_assert(sizeof(T) == 2, "16-bit storage");
     extern __shared__ __align__(128) unsigned char smem[];
 
-    const int nx = a.nx, ny = a.ny, nz = a.nz;  // nx: a power of two in [16, 256]
+    const int nx = a.nx, ny = a.ny, nz = a.nz;  // nx: a power of two in [32, 256]
     const int tiles_y = (ny + H - 1) / H;
     const int n_tiles = nz * tiles_y;
     const uint32_t pop_bytes = tma_pop_bytes<L>(nx);
@@ -482,9 +482,13 @@ template <class L, int ST, int VAR>
 bool launch_tma(const StepArgs& a, cudaStream_t stream, int* status_out)
 {
     *status_out = LBM_OK;
-    // whole rows of a power-of-two width in one box; rows of 16-byte multiples;
-    // AA: a warp's 32 pairs within one row
-    const int nx_min = VAR == LBM_PULL ? 16 : 64;
+    // Whole rows of a power-of-two width in one box; rows of 16-byte
+    // multiples. nx >= 32: a tile then holds at least 32 pairs, so every
+    // warp that reaches the warp-wide votes is full, and each staged
+    // direction (2 rows x nx x 2 bytes) is a multiple of 128 bytes, the
+    // alignment of a TMA destination in shared memory. AA: nx >= 64, a
+    // warp's 32 pairs within one row.
+    const int nx_min = VAR == LBM_PULL ? 32 : 64;
     if (a.nx < nx_min || a.nx > 256 || (a.nx & (a.nx - 1)) != 0 || a.pitch % 16 != 0) return false;
     if (reinterpret_cast<uintptr_t>(a.kind) % 16 != 0) return false;
     if (a.force_field != nullptr || !a.guo_const || a.seed == nullptr) return false;

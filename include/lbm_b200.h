@@ -129,11 +129,12 @@ typedef struct lbm_special {
  * they are one time step. Split launches let the bulk kernel keep its small
  * register budget. For float16/bfloat16 storage, LBM_LAUNCH_BULK of
  * lbm_step_pull takes the TMA-staged kernel (persistent blocks over 2-row
- * tiles, tile_x/tile_y unused) when nx is a power of two in [16, 256], pitch
+ * tiles, tile_x/tile_y unused) when nx is a power of two in [32, 256], pitch
  * is a multiple of 16, f_src and kind are 16-byte aligned, force_field is
  * NULL and round_seed is given; otherwise a kernel with two nodes per thread
  * (pitch and qstride even, no force_field), else one node per thread. All
- * three give the same bits. */
+ * three give the same bits. lbm_step_aa chooses the same way, its TMA-staged
+ * halves taking nx in [64, 256]. */
 enum { LBM_LAUNCH_FUSED = 0, LBM_LAUNCH_BULK = 1, LBM_LAUNCH_BOUNDARY = 2 };
 typedef struct lbm_launch {
     int32_t tile_x;   /* multiple of 32 */

@@ -304,6 +304,25 @@ def test_16bit_storage_matches_emulating_oracle(backend, d, storage):
     assert np.mean(a == b) > 0.7
 
 
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+@pytest.mark.parametrize("backend,nx", [("cuda-naive", 16), ("cuda-naive", 32), ("cuda-naive", 64), ("cuda-aa", 64),
+                                        ("cuda-aa", 128)])
+def test_16bit_tma_kernels_with_walls_bodies_and_rules_match_the_oracle(backend, nx, storage):
+    """Grids the TMA-staged kernels take (nx a power of two): a channel with a moving wall,
+    z walls, a Bouzidi sphere and a force, so tiles mix staged nodes, wall neighbours
+    (bounce-back with the Ladd term), rule nodes (left to the boundary warps) and warps
+    that fall back to the one-node path; several rows per warp at nx = 16 and 32.
+    Same bar as the emulating-oracle test above."""
+    body = NS.sphere(nx / 2 - 0.3, 9.6, 7.8, 4.1)
+    p, _ = cases.bouzidi(NS, 3, storage, size=(nx, 20, 16), body=body)
+    ref, gpu = run_pair(p, backend, cases.random_state(p), steps=10)
+    fluid = p.fluid
+    a, b = ref.populations()[:, fluid], gpu.populations()[:, fluid]
+    ulp = 2.0**-10 if storage == "float16" else 2.0**-7
+    assert np.abs(a - b).max() <= 4 * ulp * np.abs(a).max()
+    assert np.mean(a == b) > 0.7
+
+
 @pytest.mark.parametrize("backend", BACKENDS)
 @pytest.mark.parametrize("d", [2, 3])
 def test_fused_and_split_launches_give_identical_bits(backend, d):
