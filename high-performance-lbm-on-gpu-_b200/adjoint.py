@@ -62,16 +62,18 @@ class AdjointRun:
         axis: force component (0 = drag along x).
         checkpoint: steps between checkpoints K.
         block: bulk tile of the kernels.
+        dense_rules: link rules in the dense per-node form (``CudaSolver``); False: term by term.
     """
 
     def __init__(self, make_params, links, steps: int, window: int, axis: int = 0, checkpoint: int = 100,
-                 block=(32, 4)):
+                 block=(32, 4), dense_rules: bool = True):
         if window < 1 or window > steps:
             raise ValueError("need 1 <= window <= steps")
         self.make_params = make_params
         self.links = links
         self.steps, self.window, self.axis, self.K = int(steps), int(window), int(axis), int(checkpoint)
         self.block = block
+        self.dense_rules = bool(dense_rules)
         self._scale = None
         self.solver = None
 
@@ -92,7 +94,8 @@ class AdjointRun:
             G = np.zeros((params.d, *params.shape))
         # rule terms: those with a nonzero coefficient or a nonzero U-derivative
         keep = None if d_rules is None else np.asarray(d_rules.values.coeff) != 0.0
-        s = CudaSolver(params, variant="pull", block=self.block, force_field=G, graph=True, keep_terms=keep)
+        s = CudaSolver(params, variant="pull", block=self.block, force_field=G, graph=True, keep_terms=keep,
+                       dense_rules=self.dense_rules)
         self.solver, self.params, self.d_rules = s, params, d_rules
         self._scale = scale
         torch = s.torch

@@ -166,12 +166,14 @@ class CudaSolver(Solver):
             at immersed-boundary stencil nodes, to the node force; the immersed-boundary
             moments u* use the uniform force only, as the reference's).
         graph: capture chunks of steps in CUDA graphs (saves launch latency on small grids).
+        dense_rules: evaluate link rules in the dense per-node form (each node's distinct term
+            populations loaded once for all its rules); False: term by term.
         device: CUDA device (default: current).
     """
 
     def __init__(self, params, variant: str = "pull", block=DEFAULT_BLOCK, force_field=None,
                  graph: bool = True, device=None, pitch: int | None = None, launch: str = "split",
-                 keep_zero_terms: bool = False, keep_terms=None):
+                 keep_zero_terms: bool = False, keep_terms=None, dense_rules: bool = True):
         if variant not in VARIANTS:
             raise ValueError(f"unknown CUDA variant {variant!r}; choose from {VARIANTS}")
         if launch not in ("fused", "split"):
@@ -225,6 +227,7 @@ class CudaSolver(Solver):
         # optional mask (rules x terms, in the rules' order) of zero-coefficient
         # terms to keep: the adjoint keeps those whose U-derivative is nonzero
         self._keep_terms = None if keep_terms is None else np.asarray(keep_terms, dtype=bool)
+        self.dense_rules = bool(dense_rules)
         self._launches = {m: N.Launch(bx, by, m) for m in N.LAUNCH_MODES}
         self.block = (bx, by)
 
@@ -397,7 +400,8 @@ class CudaSolver(Solver):
             pos = np.searchsorted(nodes, export_nodes)
             np.bitwise_or.at(export_mask, pos, (np.uint32(1) << export_dirs.astype(np.uint32)))
             export_first = np.searchsorted(export_nodes, nodes, side="left").astype(np.int32)
-        if n_rules:
+        self._dense_pos = None
+        if n_rules and self.dense_rules:
             self._dense_rules(t, nodes, rule_nodes, start, term_slot, term_coeff)
         t["node"] = marked_t
         t["rule_mask"] = torch.from_numpy(rule_mask.view(np.int32)).to(self.device)
