@@ -20,7 +20,9 @@ namespace lbm {
 
 template <class L, int ST>
 __device__ __forceinline__ void ibm_moments_node(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib,
-                                                 const typename Storage<ST>::T* __restrict__ f, int layout, int n)
+                                                 const typename Storage<ST>::T* __restrict__ f, int layout, int n,
+                                                 typename Storage<ST>::R* s_rho = nullptr,
+                                                 typename Storage<ST>::R* s_us = nullptr)
 {
     using R = typename Storage<ST>::R;
     const int64_t nd = ib.node[n];
@@ -49,12 +51,18 @@ __device__ __forceinline__ void ibm_moments_node(const lbm_grid_t& g, const lbm_
         if (L::cz(k) < 0) jz -= fk;
     }
     const R rho = R(1) + drho;
+    const R u[3] = {(jx + R(0.5) * R(p.force[0])) / rho, (jy + R(0.5) * R(p.force[1])) / rho,
+                    (jz + R(0.5) * R(p.force[2])) / rho};
     R* rho_out = (R*)ib.rho;
     R* us = (R*)ib.u_star;
     rho_out[n] = rho;
-    us[n] = (jx + R(0.5) * R(p.force[0])) / rho;
-    us[ib.n_nodes + n] = (jy + R(0.5) * R(p.force[1])) / rho;
-    if (L::D == 3) us[2 * ib.n_nodes + n] = (jz + R(0.5) * R(p.force[2])) / rho;
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) us[a * ib.n_nodes + n] = u[a];
+    if (s_rho != nullptr) {
+        s_rho[n] = rho;
+#pragma unroll
+        for (int a = 0; a < L::D; ++a) s_us[a * ib.n_nodes + n] = u[a];
+    }
 }
 
 template <class L, int ST>
@@ -78,7 +86,19 @@ __global__ void ibm_moments_kernel(const lbm_grid_t g, const lbm_physics_t p, co
 template <class L> constexpr int ibm_fused_threads() { return L::D == 2 ? 1024 : 512; }
 constexpr int IBM_FUSED_MAX = 4096;
 
+// SMEM: bodies whose node and marker arrays fit in 48 KB keep a copy of
+// them in shared memory (rho, u*, the node force of the previous and the
+// current pass, the marker forces of the pass), so the phases read shared
+// memory instead of L2; the global arrays are written as well (the step,
+// the body force and the adjoint read them).
 template <class L, int ST>
+__host__ __device__ constexpr int64_t ibm_smem_reals(int nn, int nm)
+{
+    return (int64_t)nn * (1 + 3 * L::D) + (int64_t)L::D * nm;
+}
+constexpr int64_t IBM_SMEM_BYTES = 48 * 1024;
+
+template <class L, int ST, bool SMEM>
 __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel(
     const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib, const typename Storage<ST>::T* __restrict__ f,
     int layout, int iterations, typename Storage<ST>::R* force)
@@ -86,18 +106,26 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
     using R = typename Storage<ST>::R;
     constexpr int D = L::D;
     constexpr int S = D == 2 ? 9 : 27;
+    extern __shared__ __align__(16) unsigned char ibm_smem[];
     const int nn = ib.n_nodes, nm = ib.n_markers;
-    for (int n = threadIdx.x; n < nn; n += blockDim.x) ibm_moments_node<L, ST>(g, p, ib, f, layout, n);
+    R* s_rho = SMEM ? reinterpret_cast<R*>(ibm_smem) : nullptr;
+    R* s_us = SMEM ? s_rho + nn : nullptr;
+    R* s_f = SMEM ? s_us + D * nn : nullptr;  // two passes: [2][D][nn]
+    R* s_mf = SMEM ? s_f + 2 * D * nn : nullptr;
+    for (int n = threadIdx.x; n < nn; n += blockDim.x) ibm_moments_node<L, ST>(g, p, ib, f, layout, n, s_rho, s_us);
     __syncthreads();
-    const R* rho = (const R*)ib.rho;
-    const R* us = (const R*)ib.u_star;
+    const R* rho = SMEM ? s_rho : (const R*)ib.rho;
+    const R* us = SMEM ? s_us : (const R*)ib.u_star;
     const R* __restrict__ wgt = (const R*)ib.weight;
     const R* __restrict__ area = (const R*)ib.area;
     const R* __restrict__ invw = (const R*)ib.inv_weight;
     for (int it = 0; it < iterations; ++it) {
-        const R* fin = it == 0 ? nullptr : force + (int64_t)(it - 1) * D * nn;
+        const R* fin = it == 0 ? nullptr
+                               : (SMEM ? s_f + (int64_t)((it - 1) & 1) * D * nn : force + (int64_t)(it - 1) * D * nn);
         R* fout = force + (int64_t)it * D * nn;
+        R* s_fout = SMEM ? s_f + (int64_t)(it & 1) * D * nn : nullptr;
         R* mf = (R*)ib.marker_force + (int64_t)it * D * nm;
+        const R* mf_read = SMEM ? s_mf : mf;
         for (int l = threadIdx.x; l < nm; l += blockDim.x) {
             const int* st = ib.stencil + (int64_t)l * S;
             const R* wl = wgt + (int64_t)l * S;
@@ -124,7 +152,11 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
                 }
             }
 #pragma unroll
-            for (int a = 0; a < D; ++a) mf[(int64_t)a * nm + l] = R(2) * rho_l * (R(0) - U[a]) * area[l];
+            for (int a = 0; a < D; ++a) {
+                const R Fl = R(2) * rho_l * (R(0) - U[a]) * area[l];
+                mf[(int64_t)a * nm + l] = Fl;
+                if (SMEM) s_mf[a * nm + l] = Fl;
+            }
         }
         __syncthreads();
         for (int n = threadIdx.x; n < nn; n += blockDim.x) {
@@ -135,12 +167,14 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
                 const int l = ib.inv_marker[q];
                 const R wn = invw[q];
 #pragma unroll
-                for (int a = 0; a < D; ++a) acc[a] += (double)(wn * mf[(int64_t)a * nm + l]);
+                for (int a = 0; a < D; ++a) acc[a] += (double)(wn * mf_read[(int64_t)a * nm + l]);
             }
 #pragma unroll
             for (int a = 0; a < D; ++a) {
                 const double base = fin != nullptr ? (double)fin[a * nn + n] : 0.0;
-                fout[a * nn + n] = (R)(base + acc[a]);
+                const R v = (R)(base + acc[a]);
+                fout[a * nn + n] = v;
+                if (SMEM) s_fout[a * nn + n] = v;
             }
         }
         __syncthreads();
@@ -361,8 +395,15 @@ int ibm_force(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, 
     using T = typename Storage<ST>::T;
     if (ib.n_nodes <= 0) return LBM_OK;
     R* out = (R*)force;
+    const int64_t smem = ibm_smem_reals<L, ST>(ib.n_nodes, ib.n_markers) * (int64_t)sizeof(R);
+    if (smem <= IBM_SMEM_BYTES) {
+        ibm_force_fused_kernel<L, ST, true>
+            <<<1, ibm_fused_threads<L>(), (size_t)smem, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
+        return launch_status();
+    }
     if (ib.n_nodes <= IBM_FUSED_MAX && ib.n_markers <= IBM_FUSED_MAX) {
-        ibm_force_fused_kernel<L, ST><<<1, ibm_fused_threads<L>(), 0, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
+        ibm_force_fused_kernel<L, ST, false>
+            <<<1, ibm_fused_threads<L>(), 0, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
         return launch_status();
     }
     ibm_moments_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(g, p, ib, (const T*)f, layout);
