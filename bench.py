@@ -483,6 +483,24 @@ def batched_study(lbm, torch, steps: int = 640, separate_steps: int = 20):
             "steps": {"batched": steps, "separate": separate_steps}}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest value over all ranks (the slowest replica's time); x itself on one rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mlups(nodes: int, steps: int, ms: float, world: int) -> float:
+    """Whole-job MLUPS: every rank advances its own replica of `nodes` nodes by `steps` steps;
+    `ms` is the slowest rank's time."""
+    return world * nodes * steps / (ms / 1e3) / 1e6
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -527,11 +545,8 @@ def run_ours(args, rank, world, local_rank):
     ms = start.elapsed_time(stop)
     solver.time_step += warm + steps
     solver._check_health()
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    mlups = world * nodes * steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(ms, world, device)
+    mlups = whole_job_mlups(nodes, steps, ms, world)
     ms_step = ms / steps
 
     # ---- end to end through the public API, host buffers in pinned memory
@@ -553,10 +568,7 @@ def run_ours(args, rank, world, local_rank):
             fields = solver.macroscopic()
         barrier()
         dt = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([dt], dtype=torch.float64, device=device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = max_over_ranks(dt, world, device)
         h2d = 4 * nodes * 8
         d2h = 4 * nodes * fields.rho.itemsize + 16
         e2e = {"value": round(world * nodes * chunk * args.e2e_iters / dt / 1e6, 2), "unit": "MLUPS",
