@@ -282,7 +282,7 @@ def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: 
     gradients w.r.t. the inlet-speed scale U and a per-node Guo force field G ~ N(0, 1e-7^2).
 
     float32: forward and backward (recompute + adjoint kernels) timed with CUDA events, host-driven
-    as a user calls them. float64: adjoint dL/dU and dL/dG.v against central differences (h = 1e-4
+    as a user calls them; the median of three runs. float64: adjoint dL/dU and dL/dG.v against central differences (h = 1e-4
     relative).
     """
     from lbm_b200.adjoint import AdjointRun, aligned_rules
@@ -315,16 +315,21 @@ def adjoint_study(lbm, torch, steps: int = 2000, window: int = 500, checkpoint: 
     run.forward(1.0, G)  # warm-up: set-up and tables (later forwards at the same U reuse them)
     run.backward()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    torch.cuda.synchronize()
-    ev[0].record()
-    loss = run.forward(1.0, G)
-    ev[1].record()
-    dU, dG = run.backward()
-    ev[2].record()
-    ev[2].synchronize()
-    fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    fwds, bwds = [], []
+    for _ in range(3):  # the median of three forward + backward runs
+        torch.cuda.synchronize()
+        ev[0].record()
+        loss = run.forward(1.0, G)
+        ev[1].record()
+        dU, dG = run.backward()
+        ev[2].record()
+        ev[2].synchronize()
+        fwds.append(ev[0].elapsed_time(ev[1]))
+        bwds.append(ev[1].elapsed_time(ev[2]))
+    fwd, bwd = statistics.median(fwds), statistics.median(bwds)
     out["float32"] = {"loss": loss, "dL_dU": dU, "forward_ms_per_step": round(fwd / steps, 5),
-                      "backward_ms_per_step": round(bwd / steps, 5), "backward_over_forward": round(bwd / fwd, 3)}
+                      "backward_ms_per_step": round(bwd / steps, 5), "backward_over_forward": round(bwd / fwd, 3),
+                      "runs_ms": {"forward": [round(v, 2) for v in fwds], "backward": [round(v, 2) for v in bwds]}}
     if not fd:
         return out
     make64, links64, p64 = case("float64")
