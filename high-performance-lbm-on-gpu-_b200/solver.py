@@ -124,6 +124,39 @@ class Solver(ABC):
 # ---------------------------------------------------------------------------- device tables
 
 
+def dense_rule_tables(nodes, rule_nodes, start, term_key, term_coeff, max_terms: int):
+    """Dense per-node form of link rules (``lbm_special_t.ut_start``).
+
+    ``nodes``: the sorted special-node list; rule r belongs to node ``rule_nodes[r]`` and owns the
+    terms ``start[r]:start[r+1]``, each reading population ``term_key`` (a slot, or an export index)
+    with ``term_coeff``. Returns ``(ut_start, ut_key, rule_row, dense, pos)``: per node the range of
+    its rules' distinct populations, their keys, per rule the start of its coefficient row (rows
+    zero-padded to multiples of 4, so rule r of node s is
+    ``const + dense[rule_row[r] : rule_row[r] + n_s] @ values[ut_start[s] : ut_start[s+1]]``), and the
+    dense position of every term; None when a node reads more than ``max_terms`` distinct populations.
+    """
+    nodes = np.asarray(nodes)
+    counts = np.diff(np.asarray(start))
+    n_rules = counts.size
+    rule_of_term = np.repeat(np.arange(n_rules), counts)
+    s_of_rule = np.searchsorted(nodes, np.asarray(rule_nodes))
+    s_of_term = s_of_rule[rule_of_term]
+    pairs, inverse = np.unique(np.stack([s_of_term, np.asarray(term_key)], axis=1), axis=0, return_inverse=True)
+    inverse = inverse.reshape(-1)
+    ut_start = np.searchsorted(pairs[:, 0], np.arange(nodes.size + 1))
+    n_distinct = np.diff(ut_start)
+    if n_distinct.max(initial=0) > max_terms:
+        return None
+    local = inverse - ut_start[s_of_term]
+    row_len = (n_distinct[s_of_rule] + 3) // 4 * 4
+    rule_row = np.zeros(n_rules, dtype=np.int64)
+    np.cumsum(row_len[:-1], out=rule_row[1:])
+    dense = np.zeros(max(int(row_len.sum()), 4))
+    pos = rule_row[rule_of_term] + local
+    np.add.at(dense, pos, np.asarray(term_coeff, dtype=np.float64))
+    return ut_start, pairs[:, 1], rule_row, dense, pos
+
+
 PINNED_READOUT_BYTES = 1 << 30
 """Largest host readout (macroscopic fields, populations) copied through page-locked memory."""
 
@@ -412,33 +445,18 @@ class CudaSolver(Solver):
         return _SpecialTables(t, ns, n_rules, n_terms, n_export, int(ibm_nodes.size))
 
     def _dense_rules(self, t, nodes, rule_nodes, start, term_slot, term_coeff) -> None:
-        """Dense form of the rules (``lbm_special_t.ut_start``): per special node its rules' distinct terms,
-        per rule a coefficient row over them (rows padded to 4, zeros). Left out (term-by-term evaluation)
-        when a node's rules read more than ``DENSE_TERMS`` distinct populations."""
+        """Dense form of the rules on the device (``dense_rule_tables``); left out (term-by-term
+        evaluation) when a node's rules read more than ``DENSE_TERMS`` distinct populations."""
         torch = self.torch
-        counts = np.diff(start)
-        n_rules = counts.size
-        rule_of_term = np.repeat(np.arange(n_rules), counts)
-        s_of_rule = np.searchsorted(nodes, rule_nodes)
-        s_of_term = s_of_rule[rule_of_term]
-        pairs, inverse = np.unique(np.stack([s_of_term, term_slot], axis=1), axis=0, return_inverse=True)
-        inverse = inverse.reshape(-1)
-        ut_start = np.searchsorted(pairs[:, 0], np.arange(nodes.size + 1))
-        n_distinct = np.diff(ut_start)
+        tables = dense_rule_tables(nodes, rule_nodes, start, term_slot, term_coeff, N.DENSE_TERMS)
         self._dense_pos = None
-        if n_distinct.max(initial=0) > N.DENSE_TERMS:
+        if tables is None:
             return
-        local = inverse - ut_start[s_of_term]
-        row_len = (n_distinct[s_of_rule] + 3) // 4 * 4
-        rule_row = np.zeros(n_rules, dtype=np.int64)
-        np.cumsum(row_len[:-1], out=rule_row[1:])
-        dense = np.zeros(max(int(row_len.sum()), 4))
-        self._dense_pos = rule_row[rule_of_term] + local  # dense position of every live term
-        np.add.at(dense, self._dense_pos, term_coeff)
+        ut_start, ut_key, rule_row, dense, self._dense_pos = tables
         dev = self.device
         t["ut_start"] = torch.from_numpy(ut_start.astype(np.int32)).to(dev)
         key = "ut_export" if self.variant == "aa" else "ut_slot"
-        t[key] = torch.from_numpy(pairs[:, 1].astype(np.int32 if self.variant == "aa" else np.int64)).to(dev)
+        t[key] = torch.from_numpy(ut_key.astype(np.int32 if self.variant == "aa" else np.int64)).to(dev)
         t["rule_row"] = torch.from_numpy(rule_row.astype(np.int32)).to(dev)
         t["rule_dense"] = torch.from_numpy(dense).to(dev, self.t_real)
 
