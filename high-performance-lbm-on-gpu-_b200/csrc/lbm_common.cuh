@@ -221,6 +221,22 @@ __device__ __forceinline__ double v_sub(double a, double b) { return __dsub_rn(a
 __device__ __forceinline__ double v_mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double v_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ double v_rcp(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float v_neg(float a) { return -a; }
+__device__ __forceinline__ double v_neg(double a) { return -a; }
+// Two nodes at once on the packed FP32x2 pipe (FFMA2/FADD2/FMUL2): each lane
+// is the same IEEE operation as the scalar one, so a node pair updated this
+// way gets the bits of two one-node updates, with half the instructions.
+__device__ __forceinline__ float2 v_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 v_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 v_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 v_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 v_rcp(float2 a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
+__device__ __forceinline__ float2 v_neg(float2 a) { return make_float2(-a.x, -a.y); }
+// A scalar constant as a value of type V (both lanes for float2).
+template <class V> struct Splat;
+template <> struct Splat<float> { __device__ static __forceinline__ float of(float x) { return x; } };
+template <> struct Splat<double> { __device__ static __forceinline__ double of(double x) { return x; } };
+template <> struct Splat<float2> { __device__ static __forceinline__ float2 of(float x) { return make_float2(x, x); } };
 
 // ---------------------------------------------------------------- collision
 // TRT + Guo forcing on one node (reference src/lbm/collision.py:59-88,
@@ -385,13 +401,15 @@ struct NodeGuo {
     __device__ __forceinline__ R kg(int i) const { return k(i, r.g3); }
 };
 
-template <class L, class R, int SCALE_LOG2, class Guo>
-__device__ __forceinline__ void collide(R (&f)[L::Q], const Relax<R>& c, R Fx, R Fy, R Fz, const Guo& guo)
+// V: the value type -- R for one node, float2 for a node pair (R = float).
+template <class L, class R, int SCALE_LOG2, class Guo, class V>
+__device__ __forceinline__ void collide(V (&f)[L::Q], const Relax<R>& c, V Fx, V Fy, V Fz, const Guo& guo)
 {
+    using P = Splat<V>;
     constexpr double SC = (double)(1 << SCALE_LOG2);
-    R s[L::Q], d[L::Q];
-    R drho = f[0];
-    R jx = R(0), jy = R(0), jz = R(0);
+    V s[L::Q], d[L::Q];
+    V drho = f[0];
+    V jx = P::of(R(0)), jy = P::of(R(0)), jz = P::of(R(0));
     bool fx = true, fy = true, fz = true;
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
@@ -401,50 +419,69 @@ __device__ __forceinline__ void collide(R (&f)[L::Q], const Relax<R>& c, R Fx, R
         d[i] = v_sub(f[i], f[o]);
         drho = v_add(drho, s[i]);
         // j = sum c_i d over pairs (c_o = -c_i)
-        if (L::cx(i) != 0) { jx = fx ? (L::cx(i) > 0 ? d[i] : -d[i]) : (L::cx(i) > 0 ? v_add(jx, d[i]) : v_sub(jx, d[i])); fx = false; }
-        if (L::cy(i) != 0) { jy = fy ? (L::cy(i) > 0 ? d[i] : -d[i]) : (L::cy(i) > 0 ? v_add(jy, d[i]) : v_sub(jy, d[i])); fy = false; }
-        if (L::D == 3 && L::cz(i) != 0) { jz = fz ? (L::cz(i) > 0 ? d[i] : -d[i]) : (L::cz(i) > 0 ? v_add(jz, d[i]) : v_sub(jz, d[i])); fz = false; }
+        if (L::cx(i) != 0) { jx = fx ? (L::cx(i) > 0 ? d[i] : v_neg(d[i])) : (L::cx(i) > 0 ? v_add(jx, d[i]) : v_sub(jx, d[i])); fx = false; }
+        if (L::cy(i) != 0) { jy = fy ? (L::cy(i) > 0 ? d[i] : v_neg(d[i])) : (L::cy(i) > 0 ? v_add(jy, d[i]) : v_sub(jy, d[i])); fy = false; }
+        if (L::D == 3 && L::cz(i) != 0) { jz = fz ? (L::cz(i) > 0 ? d[i] : v_neg(d[i])) : (L::cz(i) > 0 ? v_add(jz, d[i]) : v_sub(jz, d[i])); fz = false; }
     }
     if (SCALE_LOG2) {
-        const R inv_sc = R(1.0 / SC);
+        const V inv_sc = P::of(R(1.0 / SC));
         drho = v_mul(drho, inv_sc);
         jx = v_mul(jx, inv_sc);
         jy = v_mul(jy, inv_sc);
         if (L::D == 3) jz = v_mul(jz, inv_sc);
     }
-    const R half = R(0.5);
-    const R rho = v_add(R(1), drho);
-    const R inv = v_rcp(rho);
-    const R ux = v_mul(v_fma(half, Fx, jx), inv);
-    const R uy = v_mul(v_fma(half, Fy, jy), inv);
-    const R uz = L::D == 3 ? v_mul(v_fma(half, Fz, jz), inv) : R(0);
-    R usq = v_mul(ux, ux);
+    const V half = P::of(R(0.5));
+    const V rho = v_add(P::of(R(1)), drho);
+    const V inv = v_rcp(rho);
+    const V ux = v_mul(v_fma(half, Fx, jx), inv);
+    const V uy = v_mul(v_fma(half, Fy, jy), inv);
+    const V uz = L::D == 3 ? v_mul(v_fma(half, Fz, jz), inv) : P::of(R(0));
+    V usq = v_mul(ux, ux);
     usq = v_fma(uy, uy, usq);
     if (L::D == 3) usq = v_fma(uz, uz, usq);
-    R uF = v_mul(ux, Fx);
+    V uF = v_mul(ux, Fx);
     uF = v_fma(uy, Fy, uF);
     if (L::D == 3) uF = v_fma(uz, Fz, uF);
     // A = w+ (drho - 1.5 rho usq) - 3 (1 - w+/2) uF
-    const R A = v_fma(c.a3m, uF, v_mul(c.wp, v_fma(v_mul(R(-1.5), rho), usq, drho)));
-    const R B = v_mul(c.b45, rho);
-    const R Dm = v_mul(c.d3, rho);
-    f[0] = v_fma(c.one_m_wp, f[0], v_mul(R(L::w(0) * SC), A));
+    const V A = v_fma(P::of(c.a3m), uF, v_mul(P::of(c.wp), v_fma(v_mul(P::of(R(-1.5)), rho), usq, drho)));
+    const V B = v_mul(P::of(c.b45), rho);
+    const V Dm = v_mul(P::of(c.d3), rho);
+    f[0] = v_fma(P::of(c.one_m_wp), f[0], v_mul(P::of(R(L::w(0) * SC)), A));
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
         const int o = L::opp(i);
         if (o < i) continue;
-        const R wi = R(L::w(i) * SC);
-        R cu = R(0);
+        const V wi = P::of(R(L::w(i) * SC));
+        V cu = P::of(R(0));
         bool first = true;
-        if (L::cx(i) != 0) { cu = L::cx(i) > 0 ? ux : -ux; first = false; }
-        if (L::cy(i) != 0) { cu = first ? (L::cy(i) > 0 ? uy : -uy) : (L::cy(i) > 0 ? v_add(cu, uy) : v_sub(cu, uy)); first = false; }
-        if (L::D == 3 && L::cz(i) != 0) cu = first ? (L::cz(i) > 0 ? uz : -uz) : (L::cz(i) > 0 ? v_add(cu, uz) : v_sub(cu, uz));
-        const R E = v_fma(cu, v_fma(v_mul(wi, B), cu, guo.kc(i)), v_mul(wi, A));
-        const R O = v_fma(v_mul(wi, Dm), cu, guo.kg(i));
-        const R P = v_fma(c.hp, s[i], E);
-        const R Qd = v_fma(c.hm, d[i], O);
-        f[i] = v_add(P, Qd);
-        f[o] = v_sub(P, Qd);
+        if (L::cx(i) != 0) { cu = L::cx(i) > 0 ? ux : v_neg(ux); first = false; }
+        if (L::cy(i) != 0) { cu = first ? (L::cy(i) > 0 ? uy : v_neg(uy)) : (L::cy(i) > 0 ? v_add(cu, uy) : v_sub(cu, uy)); first = false; }
+        if (L::D == 3 && L::cz(i) != 0) cu = first ? (L::cz(i) > 0 ? uz : v_neg(uz)) : (L::cz(i) > 0 ? v_add(cu, uz) : v_sub(cu, uz));
+        const V E = v_fma(cu, v_fma(v_mul(wi, B), cu, P::of(guo.kc(i))), v_mul(wi, A));
+        const V O = v_fma(v_mul(wi, Dm), cu, P::of(guo.kg(i)));
+        const V Pp = v_fma(P::of(c.hp), s[i], E);
+        const V Qd = v_fma(P::of(c.hm), d[i], O);
+        f[i] = v_add(Pp, Qd);
+        f[o] = v_sub(Pp, Qd);
+    }
+}
+
+// A node pair (x even, x + 1) with the uniform force on the packed FP32x2
+// pipe: fa, fb in, post-collision fa, fb out -- the bits of two one-node
+// collisions.
+template <class L, int SCALE_LOG2>
+__device__ __forceinline__ void collide_pair(float (&fa)[L::Q], float (&fb)[L::Q], const Relax<float>& c, float Fx,
+                                             float Fy, float Fz)
+{
+    float2 f[L::Q];
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) f[i] = make_float2(fa[i], fb[i]);
+    collide<L, float, SCALE_LOG2>(f, c, make_float2(Fx, Fx), make_float2(Fy, Fy), make_float2(Fz, Fz),
+                                  UniformGuo<float, SCALE_LOG2>{c});
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        fa[i] = f[i].x;
+        fb[i] = f[i].y;
     }
 }
 

@@ -437,8 +437,7 @@ struct VecPull {
         }
         const Relax<R>& rc = a.template relax<R>();
         const R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
-        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
-        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide_pair<L, S::SCALE_LOG2>(fa, fb, rc, Fx, Fy, Fz);
         const uint32_t h = sr_pair_hash(sr_pair(a.nx, a.ny, x0, y, z), a.seed[a.parity]);
         T* fd = static_cast<T*>(a.f_dst) + nd0;
 #pragma unroll
@@ -539,8 +538,7 @@ struct VecAA {
         }
         const Relax<R>& rc = a.template relax<R>();
         const R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
-        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
-        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide_pair<L, S::SCALE_LOG2>(fa, fb, rc, Fx, Fy, Fz);
         const uint32_t h = sr_pair_hash(sr_pair(a.nx, a.ny, x0, y, z), a.seed[a.parity]);
 #pragma unroll
         for (int i = 0; i < Q; ++i) {

@@ -166,8 +166,7 @@ __device__ __forceinline__ void tma_aa_pair(const StepArgs& a, const typename St
             fa[i] = S::decode_lo(w);
             fb[i] = S::decode_hi(w);
         }
-        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
-        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide_pair<L, S::SCALE_LOG2>(fa, fb, rc, Fx, Fy, Fz);
         const uint32_t h = sr_pair_hash(sr_pair(nx, ny, x0, y, z), t_seed);
         T* fd = static_cast<T*>(a.f_dst) + nd0;
 #pragma unroll
@@ -206,8 +205,7 @@ __device__ __forceinline__ void tma_aa_pair(const StepArgs& a, const typename St
                 fb[i] = S::decode_lo(row[xp]);
             }
         }
-        collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
-        collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+        collide_pair<L, S::SCALE_LOG2>(fa, fb, rc, Fx, Fy, Fz);
         const uint32_t h = sr_pair_hash(sr_pair(nx, ny, x0, y, z), t_seed);
         // the warp's 64 nodes: [x_base, x_base + 64); the nodes beyond, wrapped
         const int x_base = x0 - 2 * lane;
@@ -399,8 +397,7 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
                 // next to a wall: links from solid nodes bounce back
                 if ((k2 & KIND_NEAR) && !skip_a) bounce<L, ST>(a, fa, nd0, x0, y, z);
                 if (((k2 >> 8) & KIND_NEAR) && !skip_b) bounce<L, ST>(a, fb, nd0 + 1, x0 + 1, y, z);
-                collide<L, R, S::SCALE_LOG2>(fa, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
-                collide<L, R, S::SCALE_LOG2>(fb, rc, Fx, Fy, Fz, UniformGuo<R, S::SCALE_LOG2>{rc});
+                collide_pair<L, S::SCALE_LOG2>(fa, fb, rc, Fx, Fy, Fz);
                 const uint32_t h = sr_pair_hash(sr_pair(nx, ny, x0, y, z), t_seed);
                 T* fd = fd_base + nd0;
                 if (!skip_a && !skip_b) {
