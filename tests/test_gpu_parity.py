@@ -328,16 +328,20 @@ def test_16bit_storage_matches_emulating_oracle(backend, d, storage):
 
 
 @pytest.mark.parametrize("storage", ["float16", "bfloat16"])
-@pytest.mark.parametrize("backend,nx", [("cuda-naive", 16), ("cuda-naive", 32), ("cuda-naive", 64), ("cuda-aa", 64),
-                                        ("cuda-aa", 128)])
-def test_16bit_tma_kernels_with_walls_bodies_and_rules_match_the_oracle(backend, nx, storage):
+@pytest.mark.parametrize("backend,size", [("cuda-naive", (16, 20, 16)), ("cuda-naive", (32, 20, 16)),
+                                          ("cuda-naive", (64, 20, 16)), ("cuda-naive", (64, 21, 7)),
+                                          ("cuda-aa", (64, 20, 16)), ("cuda-aa", (128, 20, 16)),
+                                          ("cuda-aa", (64, 21, 7))])
+def test_16bit_tma_kernels_with_walls_bodies_and_rules_match_the_oracle(backend, size, storage):
     """Grids the TMA-staged kernels take (nx a power of two): a channel with a moving wall,
     z walls, a Bouzidi sphere and a force, so tiles mix staged nodes, wall neighbours
     (bounce-back with the Ladd term), rule nodes (left to the boundary warps) and warps
-    that fall back to the one-node path; several rows per warp at nx = 16 and 32.
-    Same bar as the emulating-oracle test above."""
-    body = NS.sphere(nx / 2 - 0.3, 9.6, 7.8, 4.1)
-    p, _ = cases.bouzidi(NS, 3, storage, size=(nx, 20, 16), body=body)
+    that fall back to the one-node path; several rows per warp at nx = 16 and 32 (which
+    the node-pair kernel takes), an odd row count (a last tile with one row) and a thin
+    z extent. Same bar as the emulating-oracle test above."""
+    nx, ny, nz = size
+    body = NS.sphere(nx / 2 - 0.3, (ny - 1) / 2 + 0.1, (nz - 1) / 2 + 0.2, min(4.1, (nz - 3) / 2))
+    p, _ = cases.bouzidi(NS, 3, storage, size=size, body=body)
     ref, gpu = run_pair(p, backend, cases.random_state(p), steps=10)
     fluid = p.fluid
     a, b = ref.populations()[:, fluid], gpu.populations()[:, fluid]
