@@ -16,6 +16,11 @@ ABI_VERSION = 3
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
 DENSE_TERMS = 32
+# lbm_ibm_force: one block with node and marker arrays in shared memory up to
+# IBM_SMEM_BYTES, one block on global arrays up to IBM_FUSED_MAX nodes and
+# markers, else a launch per pass (the constants of csrc/ibm.cu)
+IBM_SMEM_BYTES = 48 * 1024
+IBM_FUSED_MAX = 4096
 LBM_D2Q9, LBM_D3Q19 = 0, 1
 LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
 LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2

@@ -166,6 +166,29 @@ def test_ibm_matches_oracle(backend, d):
 
 
 @pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("radius,size,path", [(2.5, (24, 20, 20), "shared"), (4.5, (32, 24, 24), "global"),
+                                              (9.5, (48, 36, 36), "per-pass")])
+def test_every_immersed_boundary_kernel_path_matches_oracle(backend, radius, size, path):
+    """lbm_ibm_force runs bodies whose arrays fit in shared memory in one block on shared
+    memory, bodies of up to 4096 stencil nodes and markers in one block on global memory,
+    and larger ones with a launch per pass: spheres sized for each path (float64)."""
+    from lbm_b200 import _native as N
+    from lbm_b200.ibm import build_tables
+
+    nx, ny, nz = size
+    body = NS.sphere(nx / 2 - 0.3, (ny - 1) / 2 + 0.2, (nz - 1) / 2 - 0.1, radius)
+    p = cases.ibm(NS, 3, "float64", size=size, body=body)
+    t = build_tables(p.immersed, p.lattice, np.asarray(p.solid))
+    smem = (t.n_nodes * 10 + 3 * t.n_markers) * 8
+    taken = ("shared" if smem <= N.IBM_SMEM_BYTES else
+             "global" if max(t.n_nodes, t.n_markers) <= N.IBM_FUSED_MAX else "per-pass")
+    assert taken == path
+    ref, gpu = run_pair(p, backend, cases.random_state(p), steps=10)
+    assert_parity(p, ref, gpu)
+    np.testing.assert_allclose(gpu.immersed_force, ref.immersed_force, rtol=1e-13)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
 @pytest.mark.parametrize("d", [2, 3])
 def test_open_boundaries_match_oracle(backend, d):
     p, _ = cases.open_channel_case(NS, d)
