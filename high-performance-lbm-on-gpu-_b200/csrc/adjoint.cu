@@ -398,7 +398,7 @@ struct AdjointKernel {
 };
 
 template <class L, int ST>
-__global__ void __launch_bounds__(256) lbm_adjoint_bulk_kernel(const AdjArgs A)
+__global__ void __launch_bounds__(256, 4) lbm_adjoint_bulk_kernel(const AdjArgs A)
 {
     const StepArgs& a = A.a;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
