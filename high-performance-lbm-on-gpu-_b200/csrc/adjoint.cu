@@ -230,16 +230,19 @@ struct AdjointKernel {
         for (int u = 0; u < UM; ++u) slot[u] = u < n ? sp.ut_slot[u0 + u] : -1;
 #pragma unroll
         for (int u = 0; u < UM; ++u) v[u] = slot[u] >= 0 ? S::load(f + slot[u]) : R(0);
-        const R* __restrict__ dense = static_cast<const R*>(sp.rule_dense);
-        const R* __restrict__ ddense = static_cast<const R*>(A.adj.rule_ddense);
+        // the rows of the node's rules are consecutive, (n + 3) & ~3 apart
+        const int64_t row0 = sp.rule_row[rfirst];
+        const R* __restrict__ dense = static_cast<const R*>(sp.rule_dense) + row0;
+        const R* __restrict__ ddense = static_cast<const R*>(A.adj.rule_ddense) + row0;
         const R* __restrict__ rconst = static_cast<const R*>(sp.rule_const);
         const R* __restrict__ dconst = static_cast<const R*>(A.adj.rule_dconst);
+        const int n4 = (n + 3) & ~3;
         uint32_t m = rmask;
         int r = rfirst;
+        int row = 0;
         while (m) {
             const int i = __ffs(m) - 1;
             m &= m - 1u;
-            const int row = sp.rule_row[r];
             R acc = rconst[r];
             double d = with_du ? (double)dconst[r] : 0.0;
 #pragma unroll
@@ -257,6 +260,7 @@ struct AdjointKernel {
                 }
             }
             ++r;
+            row += n4;
 #pragma unroll
             for (int j = 0; j < Q; ++j)
                 if (j == i) {
@@ -377,28 +381,34 @@ struct AdjointKernel {
 #pragma unroll
             for (int j = 0; j < Q; ++j) lam[j] += acc[j * BOUNDARY_THREADS];
         }
-        finish(A, nd, s, lam, s_idx);
-        // d rule value / dU, weighted by mu of the ruled direction
+        finish(A, nd, s, lam, s_idx);  // lam now holds mu_t at x
+        // d rule value / dU, weighted by mu of the ruled direction: the
+        // node's accumulators (consecutive rules) loaded at once, then stored
         if (with_du && rmask) {
-            const R* mu = static_cast<const R*>(A.mu_out) + nd;
-            uint32_t m = rmask;
-            int r = rfirst;
-            while (m) {
-                const int i = __ffs(m) - 1;
-                m &= m - 1u;
-                double d = 0.0;
+            double* __restrict__ du = A.adj.rule_du + rfirst;
+            double old[Q];
+            int k = 0;
 #pragma unroll
-                for (int j = 0; j < Q; ++j)
-                    if (j == i) d = dv[j];
-                A.adj.rule_du[r] += (double)mu[i * qs] * d;
-                ++r;
-            }
+            for (int i = 0; i < Q; ++i)
+                if ((rmask >> i) & 1u) old[i] = du[k++];
+            k = 0;
+#pragma unroll
+            for (int i = 0; i < Q; ++i)
+                if ((rmask >> i) & 1u) du[k++] = __fma_rn((double)lam[i], dv[i], old[i]);
         }
     }
 };
 
+// 4 resident blocks of 256 (64 registers) for 4-byte reals, where that costs
+// a few bytes of spill; float64 would spill ~900 bytes per thread there.
+template <int ST>
+constexpr int adjoint_bulk_min_blocks()
+{
+    return sizeof(typename Storage<ST>::R) == 4 ? 4 : 1;
+}
+
 template <class L, int ST>
-__global__ void __launch_bounds__(256, 4) lbm_adjoint_bulk_kernel(const AdjArgs A)
+__global__ void __launch_bounds__(256, adjoint_bulk_min_blocks<ST>()) lbm_adjoint_bulk_kernel(const AdjArgs A)
 {
     const StepArgs& a = A.a;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;

@@ -137,14 +137,15 @@ struct StepKernel {
 #pragma unroll
             for (int u = 0; u < UM; ++u) v[u] = e[u] >= 0 ? ex[e[u]] : R(0);
         }
-        const R* __restrict__ dense = static_cast<const R*>(sp.rule_dense);
+        // the rows of the node's rules are consecutive, (n + 3) & ~3 apart
+        const R* __restrict__ row = static_cast<const R*>(sp.rule_dense) + sp.rule_row[rfirst];
         const R* __restrict__ rconst = static_cast<const R*>(sp.rule_const);
+        const int n4 = (n + 3) & ~3;
         uint32_t m = rmask;
         int r = rfirst;
         while (m) {
             const int i = __ffs(m) - 1;
             m &= m - 1u;
-            const R* row = dense + sp.rule_row[r];
             R acc = rconst[r++];
 #pragma unroll
             for (int u = 0; u < UM; u += 4) {
@@ -155,6 +156,7 @@ struct StepKernel {
                     for (int k = 0; k < 4; ++k) acc = v_fma(c[k], v[u + k], acc);
                 }
             }
+            row += n4;
 #pragma unroll
             for (int j = 0; j < Q; ++j)
                 if (j == i) f[j] = acc;

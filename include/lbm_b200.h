@@ -108,7 +108,9 @@ typedef struct lbm_special {
     const int32_t* ut_start;      /* n_special + 1 */
     const int64_t* ut_slot;       /* pull: slot (dir * qstride + pitched node) of each distinct term */
     const int32_t* ut_export;     /* AA: export index of each distinct term */
-    const int32_t* rule_row;      /* n_rules: start of rule r's row, a multiple of 4 */
+    const int32_t* rule_row;      /* n_rules: start of rule r's row, a multiple of 4; the rows of one
+                                     node's rules are consecutive, each (n + 3) & ~3 long (n: the node's
+                                     distinct populations), and the kernels read the first one only */
     const void* rule_dense;       /* real, 16-byte aligned; rows zero-padded to multiples of 4 */
 } lbm_special_t;
 
