@@ -16,9 +16,10 @@ ABI_VERSION = 3
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
 DENSE_TERMS = 32
-# lbm_ibm_force: one block with node and marker arrays in shared memory up to
-# IBM_SMEM_BYTES, one block on global arrays up to IBM_FUSED_MAX nodes and
-# markers, else a launch per pass (the constants of csrc/ibm.cu)
+# lbm_ibm_force: one block with node and marker arrays (and, when they fit
+# too, the body's tables) in shared memory up to IBM_SMEM_BYTES, one block on
+# global arrays up to IBM_FUSED_MAX nodes and markers, else a launch per pass
+# (the constants of csrc/ibm.cu)
 IBM_SMEM_BYTES = 48 * 1024
 IBM_FUSED_MAX = 4096
 LBM_D2Q9, LBM_D3Q19 = 0, 1

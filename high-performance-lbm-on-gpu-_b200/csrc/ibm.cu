@@ -86,19 +86,32 @@ __global__ void ibm_moments_kernel(const lbm_grid_t g, const lbm_physics_t p, co
 template <class L> constexpr int ibm_fused_threads() { return L::D == 2 ? 1024 : 512; }
 constexpr int IBM_FUSED_MAX = 4096;
 
-// SMEM: bodies whose node and marker arrays fit in 48 KB keep a copy of
+// MODE 1: bodies whose node and marker arrays fit in 48 KB keep a copy of
 // them in shared memory (rho, u*, the node force of the previous and the
 // current pass, the marker forces of the pass), so the phases read shared
 // memory instead of L2; the global arrays are written as well (the step,
-// the body force and the adjoint read them).
+// the body force and the adjoint read them). MODE 2: when the body's tables
+// (stencils, weights, areas, the inverse CSR) fit beside them, they are
+// copied in too, all with independent loads in one phase, and the passes
+// make no global load at all. MODE 0: everything in global memory.
 template <class L, int ST>
 __host__ __device__ constexpr int64_t ibm_smem_reals(int nn, int nm)
 {
     return (int64_t)nn * (1 + 3 * L::D) + (int64_t)L::D * nm;
 }
+// The tables: real weight[nm S], area[nm], inv_weight[nm S], then int32
+// stencil[nm S], inv_start[nn + 1], inv_marker[nm S] (the inverse CSR lists
+// every (marker, stencil position) pair once: nm S entries).
+template <class L, int ST>
+__host__ __device__ constexpr int64_t ibm_table_bytes(int nn, int nm)
+{
+    constexpr int64_t S = L::D == 2 ? 9 : 27;
+    using R = typename Storage<ST>::R;
+    return ((int64_t)nm * (2 * S + 1)) * (int64_t)sizeof(R) + ((int64_t)nm * 2 * S + nn + 1) * 4;
+}
 constexpr int64_t IBM_SMEM_BYTES = 48 * 1024;
 
-template <class L, int ST, bool SMEM>
+template <class L, int ST, int MODE>
 __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel(
     const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib, const typename Storage<ST>::T* __restrict__ f,
     int layout, int iterations, typename Storage<ST>::R* force)
@@ -106,19 +119,60 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
     using R = typename Storage<ST>::R;
     constexpr int D = L::D;
     constexpr int S = D == 2 ? 9 : 27;
+    constexpr bool SMEM = MODE >= 1;
     extern __shared__ __align__(16) unsigned char ibm_smem[];
     const int nn = ib.n_nodes, nm = ib.n_markers;
     R* s_rho = SMEM ? reinterpret_cast<R*>(ibm_smem) : nullptr;
     R* s_us = SMEM ? s_rho + nn : nullptr;
     R* s_f = SMEM ? s_us + D * nn : nullptr;  // two passes: [2][D][nn]
     R* s_mf = SMEM ? s_f + 2 * D * nn : nullptr;
+    const int* stencil = ib.stencil;
+    const R* wgt = (const R*)ib.weight;
+    const R* area = (const R*)ib.area;
+    const int* inv_start = ib.inv_start;
+    const int* inv_marker = ib.inv_marker;
+    const R* invw = (const R*)ib.inv_weight;
+    if constexpr (MODE == 2) {
+        const int pairs = nm * S;
+        R* t_w = s_mf + D * nm;
+        R* t_area = t_w + pairs;
+        R* t_invw = t_area + nm;
+        int* t_st = reinterpret_cast<int*>(t_invw + pairs);
+        int* t_is = t_st + pairs;
+        int* t_im = t_is + nn + 1;
+        const int count = pairs > nn + 1 ? pairs : nn + 1;
+        for (int i = threadIdx.x; i < count; i += blockDim.x) {
+            // every load of the entry first, then the stores: one round trip
+            int st = 0, im = 0, is = 0;
+            R w = R(0), iw = R(0), ar = R(0);
+            if (i < pairs) {
+                st = ib.stencil[i];
+                w = wgt[i];
+                im = ib.inv_marker[i];
+                iw = invw[i];
+            }
+            if (i <= nn) is = ib.inv_start[i];
+            if (i < nm) ar = area[i];
+            if (i < pairs) {
+                t_st[i] = st;
+                t_w[i] = w;
+                t_im[i] = im;
+                t_invw[i] = iw;
+            }
+            if (i <= nn) t_is[i] = is;
+            if (i < nm) t_area[i] = ar;
+        }
+        stencil = t_st;
+        wgt = t_w;
+        area = t_area;
+        inv_start = t_is;
+        inv_marker = t_im;
+        invw = t_invw;
+    }
     for (int n = threadIdx.x; n < nn; n += blockDim.x) ibm_moments_node<L, ST>(g, p, ib, f, layout, n, s_rho, s_us);
     __syncthreads();
     const R* rho = SMEM ? s_rho : (const R*)ib.rho;
     const R* us = SMEM ? s_us : (const R*)ib.u_star;
-    const R* __restrict__ wgt = (const R*)ib.weight;
-    const R* __restrict__ area = (const R*)ib.area;
-    const R* __restrict__ invw = (const R*)ib.inv_weight;
     for (int it = 0; it < iterations; ++it) {
         const R* fin = it == 0 ? nullptr
                                : (SMEM ? s_f + (int64_t)((it - 1) & 1) * D * nn : force + (int64_t)(it - 1) * D * nn);
@@ -127,7 +181,7 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
         R* mf = (R*)ib.marker_force + (int64_t)it * D * nm;
         const R* mf_read = SMEM ? s_mf : mf;
         for (int l = threadIdx.x; l < nm; l += blockDim.x) {
-            const int* st = ib.stencil + (int64_t)l * S;
+            const int* st = stencil + (int64_t)l * S;
             const R* wl = wgt + (int64_t)l * S;
             int m[S];
             R w[S];
@@ -163,8 +217,8 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
             double acc[D];
 #pragma unroll
             for (int a = 0; a < D; ++a) acc[a] = 0.0;
-            for (int q = ib.inv_start[n]; q < ib.inv_start[n + 1]; ++q) {
-                const int l = ib.inv_marker[q];
+            for (int q = inv_start[n]; q < inv_start[n + 1]; ++q) {
+                const int l = inv_marker[q];
                 const R wn = invw[q];
 #pragma unroll
                 for (int a = 0; a < D; ++a) acc[a] += (double)(wn * mf_read[(int64_t)a * nm + l]);
@@ -396,13 +450,19 @@ int ibm_force(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, 
     if (ib.n_nodes <= 0) return LBM_OK;
     R* out = (R*)force;
     const int64_t smem = ibm_smem_reals<L, ST>(ib.n_nodes, ib.n_markers) * (int64_t)sizeof(R);
+    const int64_t with_tables = smem + ibm_table_bytes<L, ST>(ib.n_nodes, ib.n_markers);
+    if (with_tables <= IBM_SMEM_BYTES) {
+        ibm_force_fused_kernel<L, ST, 2>
+            <<<1, ibm_fused_threads<L>(), (size_t)with_tables, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
+        return launch_status();
+    }
     if (smem <= IBM_SMEM_BYTES) {
-        ibm_force_fused_kernel<L, ST, true>
+        ibm_force_fused_kernel<L, ST, 1>
             <<<1, ibm_fused_threads<L>(), (size_t)smem, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
         return launch_status();
     }
     if (ib.n_nodes <= IBM_FUSED_MAX && ib.n_markers <= IBM_FUSED_MAX) {
-        ibm_force_fused_kernel<L, ST, false>
+        ibm_force_fused_kernel<L, ST, 0>
             <<<1, ibm_fused_threads<L>(), 0, s>>>(g, p, ib, (const T*)f, layout, iterations, out);
         return launch_status();
     }

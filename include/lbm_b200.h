@@ -263,7 +263,9 @@ typedef struct lbm_ibm {
     const int32_t* stencil;    /* [n_markers][stencil_size] positions in node[] */
     const void* weight;        /* real[n_markers][stencil_size] Roma weights */
     const void* area;          /* real[n_markers] */
-    const int32_t* inv_start;  /* [n_nodes + 1] CSR over (marker, weight) pairs per node */
+    const int32_t* inv_start;  /* [n_nodes + 1] CSR over (marker, weight) pairs per node; every
+                                  (marker, stencil position) appears once: inv_start[n_nodes] ==
+                                  n_markers * stencil_size */
     const int32_t* inv_marker;
     const void* inv_weight;    /* real */
     void* rho;                 /* real[n_nodes] scratch */

@@ -166,12 +166,13 @@ def test_ibm_matches_oracle(backend, d):
 
 
 @pytest.mark.parametrize("backend", BACKENDS)
-@pytest.mark.parametrize("radius,size,path", [(2.5, (24, 20, 20), "shared"), (4.5, (32, 24, 24), "global"),
-                                              (9.5, (48, 36, 36), "per-pass")])
+@pytest.mark.parametrize("radius,size,path", [(1.5, (24, 20, 20), "tables"), (2.5, (24, 20, 20), "shared"),
+                                              (4.5, (32, 24, 24), "global"), (9.5, (48, 36, 36), "per-pass")])
 def test_every_immersed_boundary_kernel_path_matches_oracle(backend, radius, size, path):
-    """lbm_ibm_force runs bodies whose arrays fit in shared memory in one block on shared
-    memory, bodies of up to 4096 stencil nodes and markers in one block on global memory,
-    and larger ones with a launch per pass: spheres sized for each path (float64)."""
+    """lbm_ibm_force runs a body in one block with its arrays and tables in shared memory
+    when both fit, with its arrays alone there when they fit, in one block on global
+    memory up to 4096 stencil nodes and markers, and with a launch per pass beyond:
+    spheres sized for each path (float64)."""
     from lbm_b200 import _native as N
     from lbm_b200.ibm import build_tables
 
@@ -180,7 +181,8 @@ def test_every_immersed_boundary_kernel_path_matches_oracle(backend, radius, siz
     p = cases.ibm(NS, 3, "float64", size=size, body=body)
     t = build_tables(p.immersed, p.lattice, np.asarray(p.solid))
     smem = (t.n_nodes * 10 + 3 * t.n_markers) * 8
-    taken = ("shared" if smem <= N.IBM_SMEM_BYTES else
+    tables = t.n_markers * 55 * 8 + (t.n_markers * 54 + t.n_nodes + 1) * 4
+    taken = ("tables" if smem + tables <= N.IBM_SMEM_BYTES else "shared" if smem <= N.IBM_SMEM_BYTES else
              "global" if max(t.n_nodes, t.n_markers) <= N.IBM_FUSED_MAX else "per-pass")
     assert taken == path
     ref, gpu = run_pair(p, backend, cases.random_state(p), steps=10)
