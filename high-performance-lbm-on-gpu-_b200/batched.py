@@ -108,8 +108,9 @@ class BatchedSolver:
                     continue
                 n = g.nx * g.ny * g.nz
                 wall = np.asarray(self.params[i].wall_velocity, dtype=np.float64).reshape(d, n)
+                # a writable copy: the parameters' arrays are read-only
                 self._wall[w0 : w0 + d * g.qstride].view(d, g.qstride)[:, :n] = torch.from_numpy(
-                    np.ascontiguousarray(wall)).to(self.device, self.t_real)
+                    np.array(wall, copy=True)).to(self.device, self.t_real)
 
         # ---- node kinds and solid-neighbour masks, domain by domain
         self._nbr = torch.zeros(koff, dtype=torch.int32, device=self.device)
