@@ -304,6 +304,8 @@ class CudaSolver(Solver):
         """(..., *shape) host array -> device tensor (..., qstride), zero padding columns."""
         torch = self.torch
         host = np.ascontiguousarray(host)
+        if not host.flags.writeable:  # the parameters' arrays are read-only; torch wants a writable buffer
+            host = host.copy()
         lead = host.shape[: host.ndim - len(self.shape)]
         t = torch.from_numpy(host).to(self.device, dtype)
         if self.pitch == self.shape[-1]:
