@@ -18,8 +18,9 @@ product package never loads them.
 
 The launchers mirror ``CudaSolver._advance`` (``cuda_solver.py:267-284``):
 grid (ceil(nx/bx), ceil(ny/by), nz), block (bx, by), default block (32, 8);
-``stream_collide_naive`` between two buffers; ``aa_odd`` then ``aa_even`` on
-one buffer that starts in the post-even layout (slot opp(i) holds f_i).
+``stream_collide_naive`` (and, 2D only, ``stream_collide_tiled``, whose block
+is its tile) between two buffers; ``aa_odd`` then ``aa_even`` on one buffer
+that starts in the post-even layout (slot opp(i) holds f_i).
 """
 
 from __future__ import annotations
@@ -69,6 +70,21 @@ extern "C" int ref_step_aa(void* f, int odd, const unsigned char* solid, const v
 }
 """
 
+# 2D only: the tiled kernel's block must be its tile (TILE_X x TILE_Y)
+_TILED_LAUNCHER = r"""
+extern "C" int ref_step_tiled(const void* f_src, void* f_dst, const unsigned char* solid, const void* wall_u,
+                              const void* force_field, int nx, int ny, int nz, double omega_plus,
+                              double omega_minus, double fx, double fy, double fz, int bx, int by, void* stream)
+{
+    if (bx != TILE_X || by != TILE_Y || nz != 1) return (int)cudaErrorInvalidValue;
+    const dim3 grid((nx + bx - 1) / bx, (ny + by - 1) / by, 1), block(bx, by, 1);
+    stream_collide_tiled<<<grid, block, 0, (cudaStream_t)stream>>>(
+        (const real_t*)f_src, (real_t*)f_dst, solid, (const real_t*)wall_u, (const real_t*)force_field, nx, ny, nz,
+        (real_t)omega_plus, (real_t)omega_minus, (real_t)fx, (real_t)fy, (real_t)fz);
+    return (int)cudaGetLastError();
+}
+"""
+
 
 def library_path(lattice: str, dtype: str) -> Path:
     return OUT / f"libref_{lattice}_{dtype}.so"
@@ -104,7 +120,9 @@ def build(verbose: bool = False) -> bool:
                 f'#include "{KERNELS / "common.cuh"}"',
                 f'#include "{KERNELS / "stream_collide_naive.cu"}"',
                 f'#include "{KERNELS / "stream_collide_aa.cu"}"',
+                f'#include "{KERNELS / "stream_collide_tiled.cu"}"' if lat == "D2Q9" else "",
                 _LAUNCHERS,
+                _TILED_LAUNCHER if lat == "D2Q9" else "",
             ]))
             target = library_path(lat, dtype)
             cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-shared",
@@ -132,6 +150,9 @@ class RefKernels:
         lib.ref_step_naive.restype = c.c_int
         lib.ref_step_aa.argtypes = [c.c_void_p, c.c_int] + common
         lib.ref_step_aa.restype = c.c_int
+        if lattice == "D2Q9":
+            lib.ref_step_tiled.argtypes = [c.c_void_p, c.c_void_p] + common
+            lib.ref_step_tiled.restype = c.c_int
         self.lib = lib
 
 
@@ -143,6 +164,11 @@ class RefSolver:
     def __init__(self, params, variant: str = "naive", block=DEFAULT_BLOCK, device="cuda"):
         import numpy as np
         import torch
+
+        if variant not in ("naive", "tiled", "aa") or (variant == "tiled" and params.d != 2):
+            raise ValueError(f"variant {variant!r} is not available for a {params.d}D grid")
+        if variant == "tiled" and tuple(block) != DEFAULT_BLOCK:
+            raise ValueError(f"the tiled kernel is compiled for blocks of {DEFAULT_BLOCK}")
 
         self.torch = torch
         self.params = params
@@ -187,9 +213,10 @@ class RefSolver:
                     if err:
                         raise RuntimeError(f"reference AA kernel launch failed ({err})")
         else:
+            step = lib.ref_step_tiled if self.variant == "tiled" else lib.ref_step_naive
             for _ in range(steps):
-                err = lib.ref_step_naive(self.f.data_ptr(), self.f_next.data_ptr(), self.solid.data_ptr(),
-                                         self.wall.data_ptr(), self.field.data_ptr(), *self.scalars, bx, by, stream)
+                err = step(self.f.data_ptr(), self.f_next.data_ptr(), self.solid.data_ptr(),
+                           self.wall.data_ptr(), self.field.data_ptr(), *self.scalars, bx, by, stream)
                 if err:
                     raise RuntimeError(f"reference kernel launch failed ({err})")
                 self.f, self.f_next = self.f_next, self.f
@@ -206,7 +233,7 @@ def _time_pair(lbm, torch, params, steps: int, variant: str):
     that step count exist before the timed run)."""
     import numpy as np
 
-    backend = "cuda-aa" if variant == "aa" else "cuda-naive"
+    backend = "cuda-aa" if variant == "aa" else "cuda-naive"  # tiled: against this build's pull step
     ours = lbm.make_solver(params, backend=backend)
     ours.initialize()
     ref = RefSolver(params, variant)
@@ -242,7 +269,7 @@ def main() -> None:
     tgv = lbm.SimulationParams(nx=2048, ny=2048, tau=0.8, collision="trt", dtype="float32")
     result = {
         "duct_256_d3q19_float32": {v: _time_pair(lbm, torch, duct, 200, v) for v in ("naive", "aa")},
-        "periodic_2048_d2q9_float32": {v: _time_pair(lbm, torch, tgv, 400, v) for v in ("naive", "aa")},
+        "periodic_2048_d2q9_float32": {v: _time_pair(lbm, torch, tgv, 400, v) for v in ("naive", "tiled", "aa")},
         "unit": "MLUPS (all nodes, CUDA events, inputs larger than L2)",
         "device": torch.cuda.get_device_name(0),
     }

@@ -51,6 +51,24 @@ def test_step_matches_the_reference_kernels(d, collision, dtype, variant):
     assert np.isfinite(a).all() and np.abs(a).max() > 1e-4  # the flow is not trivial
 
 
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_pull_step_matches_the_reference_tiled_kernel(dtype):
+    """The reference's shared-memory tiled kernel (2D only) on the 2D mixed case."""
+    p = cases.mixed(NS, dtype, "trt", 2)
+    start = OracleSolver(p)
+    start.initialize(*cases.random_state(p))
+    f0 = start.populations()
+    ref = ref_kernels.RefSolver(p, "tiled")
+    ref.set_populations(f0)
+    ours = lbm.make_solver(p, backend="cuda-naive")
+    ours.set_populations(f0)
+    ref.advance(cases.EQUIVALENCE_STEPS)
+    ours.run(cases.EQUIVALENCE_STEPS)
+    fluid = p.fluid
+    diff = float(np.abs(ref.populations()[:, fluid] - ours.populations()[:, fluid]).max())
+    assert diff < ABS[dtype], diff
+
+
 @pytest.mark.parametrize("block", [(32, 8), (64, 4), (16, 16)])
 def test_reference_launch_shapes_agree_with_ours_on_the_duct(block):
     """The reference's block shape changes nothing; a 64^3 duct (walls in y and z, force)

@@ -20,5 +20,5 @@ def test_reference_kernel_library_exports_its_launchers(lattice, dtype):
         lib = ctypes.CDLL(str(ref_kernels.library_path(lattice, dtype)))
     except OSError as e:  # the CUDA runtime may be absent without a driver
         pytest.skip(f"cannot load without the CUDA driver: {e}")
-    for name in ("ref_step_naive", "ref_step_aa"):
+    for name in ("ref_step_naive", "ref_step_aa") + (("ref_step_tiled",) if lattice == "D2Q9" else ()):
         assert hasattr(lib, name)
