@@ -276,7 +276,28 @@ def main() -> None:
     print(json.dumps(result), flush=True)
 
 
+def small_case(steps: int = 10) -> None:
+    """A profiling case: the reference's pull kernel alone on a 128^3 duct in float32
+    (2 x 159 MB of populations, larger than L2), `steps` launches."""
+    import torch
+
+    sys.path.insert(0, str(HERE.parent))
+    import lbm_b200 as lbm
+
+    n = 128
+    p = lbm.SimulationParams(nx=n, ny=n, nz=n, tau=0.9, collision="trt", force=(1e-6, 0.0, 0.0),
+                             solid=lbm.duct_walls(n, n, n), dtype="float32")
+    ref = RefSolver(p, "naive")
+    ref.set_populations(torch.zeros((p.lattice.q, *p.shape), dtype=torch.float32))
+    ref.advance(steps)
+    torch.cuda.synchronize()
+    print(f"reference stream_collide_naive: {steps} steps on a {n}^3 duct")
+
+
 if __name__ == "__main__":
     if "--build" in sys.argv:
         sys.exit(0 if build(verbose=True) else 1)
-    main()
+    if "--small" in sys.argv:
+        small_case()
+    else:
+        main()
