@@ -20,7 +20,9 @@ The launchers mirror ``CudaSolver._advance`` (``cuda_solver.py:267-284``):
 grid (ceil(nx/bx), ceil(ny/by), nz), block (bx, by), default block (32, 8);
 ``stream_collide_naive`` (and, 2D only, ``stream_collide_tiled``, whose block
 is its tile) between two buffers; ``aa_odd`` then ``aa_even`` on one buffer
-that starts in the post-even layout (slot opp(i) holds f_i).
+that starts in the post-even layout (slot opp(i) holds f_i); before every
+launch the link-rule pre-pass of that launch's layout (``rules_evaluate``,
+``rules_write`` from ``kernels/link_rules.cu``), as ``_pre_pass`` runs it.
 """
 
 from __future__ import annotations
@@ -66,6 +68,27 @@ extern "C" int ref_step_aa(void* f, int odd, const unsigned char* solid, const v
         aa_even<<<grid, block, 0, (cudaStream_t)stream>>>((real_t*)f, solid, (const real_t*)force_field, nx, ny, nz,
                                                           (real_t)omega_plus, (real_t)omega_minus, (real_t)fx,
                                                           (real_t)fy, (real_t)fz);
+    return (int)cudaGetLastError();
+}
+"""
+
+# the link-rule pre-pass (kernels/link_rules.cu needs only real_t), launched as
+# _RulePass launches it: RULES_BLOCK threads per block (cuda_solver.py:98-176)
+_RULE_LAUNCHERS = r"""
+extern "C" int ref_rules_evaluate(const void* f, const long long* slot, const void* coeff, const void* constant,
+                                  void* out, int n_rules, int n_terms, void* stream)
+{
+    if (n_rules <= 0) return 0;
+    rules_evaluate<<<(n_rules + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+        (const real_t*)f, slot, (const real_t*)coeff, (const real_t*)constant, (real_t*)out, n_rules, n_terms);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ref_rules_write(void* f, const long long* target, const void* value, int n_rules, void* stream)
+{
+    if (n_rules <= 0) return 0;
+    rules_write<<<(n_rules + 127) / 128, 128, 0, (cudaStream_t)stream>>>((real_t*)f, target, (const real_t*)value,
+                                                                        n_rules);
     return (int)cudaGetLastError();
 }
 """
@@ -121,7 +144,9 @@ def build(verbose: bool = False) -> bool:
                 f'#include "{KERNELS / "stream_collide_naive.cu"}"',
                 f'#include "{KERNELS / "stream_collide_aa.cu"}"',
                 f'#include "{KERNELS / "stream_collide_tiled.cu"}"' if lat == "D2Q9" else "",
+                f'#include "{KERNELS / "link_rules.cu"}"',
                 _LAUNCHERS,
+                _RULE_LAUNCHERS,
                 _TILED_LAUNCHER if lat == "D2Q9" else "",
             ]))
             target = library_path(lat, dtype)
@@ -153,7 +178,59 @@ class RefKernels:
         if lattice == "D2Q9":
             lib.ref_step_tiled.argtypes = [c.c_void_p, c.c_void_p] + common
             lib.ref_step_tiled.restype = c.c_int
+        lib.ref_rules_evaluate.argtypes = [c.c_void_p] * 5 + [c.c_int, c.c_int, c.c_void_p]
+        lib.ref_rules_evaluate.restype = c.c_int
+        lib.ref_rules_write.argtypes = [c.c_void_p] * 3 + [c.c_int, c.c_void_p]
+        lib.ref_rules_write.restype = c.c_int
         self.lib = lib
+
+
+class RulePass:
+    """The reference's link-rule pre-pass for one layout (``_RulePass``, ``cuda_solver.py:114-176``):
+    rules compiled to flat slots of the layout, grouped by their number of non-zero terms, each
+    group trimmed to that length and stored term-major, evaluated group by group into one buffer,
+    then written back by one launch. Slots come from this package's ``compile_rules``, which
+    follows the reference's ``compile_rules`` (``link_rules.py:203-250``)."""
+
+    def __init__(self, params, layout: str, kernels: RefKernels, torch, device, t_real):
+        import numpy as np
+
+        from lbm_b200.link_rules import compile_rules
+
+        compiled = compile_rules(params.lattice, params.link_rules, layout, params.solid, params.wall_velocity)
+        values = compiled.values
+        lengths = np.count_nonzero(values.coeff, axis=1)
+        order = np.argsort(lengths, kind="stable")
+        self.groups = []
+        start = 0
+        for length in np.unique(lengths):
+            rows = order[lengths[order] == length]
+            nonzero_first = np.argsort(values.coeff[rows] == 0, axis=1, kind="stable")
+            take = nonzero_first[:, : max(int(length), 1)]
+            slots = np.take_along_axis(values.slots[rows], take, axis=1)
+            coeff = np.take_along_axis(values.coeff[rows], take, axis=1)
+            self.groups.append((
+                start, len(rows),
+                torch.from_numpy(np.ascontiguousarray(slots.T).astype(np.int64)).to(device),
+                torch.from_numpy(np.ascontiguousarray(coeff.T)).to(device, t_real),
+                torch.from_numpy(np.array(values.constant[rows])).to(device, t_real),
+            ))
+            start += len(rows)
+        self.target = torch.from_numpy(np.array(compiled.target[order], dtype=np.int64)).to(device)
+        self.buffer = torch.empty(len(order), dtype=t_real, device=device)
+        self.n = len(order)
+        self.lib = kernels.lib
+        self.itemsize = self.buffer.element_size()
+
+    def __call__(self, f, stream) -> None:
+        base = self.buffer.data_ptr()
+        for start, count, slots, coeff, constant in self.groups:
+            err = self.lib.ref_rules_evaluate(f.data_ptr(), slots.data_ptr(), coeff.data_ptr(), constant.data_ptr(),
+                                              base + start * self.itemsize, count, slots.shape[0], stream)
+            if err:
+                raise RuntimeError(f"reference rule evaluation failed ({err})")
+        if self.lib.ref_rules_write(f.data_ptr(), self.target.data_ptr(), base, self.n, stream):
+            raise RuntimeError("reference rule write-back failed")
 
 
 class RefSolver:
@@ -182,6 +259,12 @@ class RefSolver:
         self.solid = torch.from_numpy(np.asarray(params.solid, dtype=np.uint8).copy()).to(device)
         self.wall = torch.from_numpy(np.array(params.wall_velocity, dtype=np.float64)).to(device, t_real).contiguous()
         self.field = torch.zeros(1, dtype=t_real, device=device)
+        self.rule_passes = {}
+        if getattr(params, "link_rules", None) is not None and len(params.link_rules):
+            layouts = ("aa_odd", "aa_even") if variant == "aa" else ("pull",)
+            self.rule_passes = {lay: RulePass(params, lay, self.kernels, torch, device, t_real) for lay in layouts}
+        if getattr(params, "immersed", None) is not None:
+            raise ValueError("the reference drives immersed bodies with CuPy array code, not with these kernels")
         self.scalars = (params.nx, params.ny, params.nz or 1, *params.relaxation_rates,
                         *(tuple(float(v) for v in params.force) + (0.0,) * (3 - params.d))[:3])
         self.f = self.f_next = None
@@ -208,6 +291,8 @@ class RefSolver:
                 raise ValueError("the AA kernels advance in pairs of steps")
             for _ in range(steps // 2):
                 for odd in (1, 0):
+                    if self.rule_passes:
+                        self.rule_passes["aa_odd" if odd else "aa_even"](self.f, stream)
                     err = lib.ref_step_aa(p(), odd, self.solid.data_ptr(), self.wall.data_ptr(),
                                           self.field.data_ptr(), *self.scalars, bx, by, stream)
                     if err:
@@ -215,6 +300,8 @@ class RefSolver:
         else:
             step = lib.ref_step_tiled if self.variant == "tiled" else lib.ref_step_naive
             for _ in range(steps):
+                if self.rule_passes:
+                    self.rule_passes["pull"](self.f, stream)
                 err = step(self.f.data_ptr(), self.f_next.data_ptr(), self.solid.data_ptr(),
                            self.wall.data_ptr(), self.field.data_ptr(), *self.scalars, bx, by, stream)
                 if err:

@@ -1,8 +1,9 @@
 """The CUDA path against the reference's own CUDA kernels on the same B200 (GPU).
 
 ``oracle/ref_kernels.py`` compiles the reference's ``stream_collide_naive``,
-``aa_odd`` and ``aa_even`` (``src/lbm/backends/kernels/*.cu``) unmodified for
-sm_100a and drives them as the reference's ``CudaSolver`` does. Both sides
+``aa_odd``, ``aa_even``, ``stream_collide_tiled`` (2D) and its link-rule
+pre-pass (``src/lbm/backends/kernels/*.cu``) unmodified for sm_100a and drives
+them as the reference's ``CudaSolver`` does. Both sides
 start from the same populations (the oracle's initial state, restored
 population-exactly) and advance 40 steps of the reference's mixed-geometry
 case: walls, a moving wall, an obstacle and a body force. Bounds: those of the
@@ -49,6 +50,33 @@ def test_step_matches_the_reference_kernels(d, collision, dtype, variant):
     diff = float(np.abs(a - b).max())
     assert diff < ABS[dtype], diff
     assert np.isfinite(a).all() and np.abs(a).max() > 1e-4  # the flow is not trivial
+
+
+@pytest.mark.parametrize("variant", ["naive", "aa"])
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("case", ["bouzidi", "zou_he"])
+@pytest.mark.parametrize("d", [2, 3])
+def test_link_rules_match_the_reference_rule_prepass(d, case, dtype, variant):
+    """Bouzidi bodies (with a moving wall and a force) and Zou-He inlet/outlet: this build
+    evaluates the rules inside its step; the reference runs its rule pre-pass kernels
+    (rules_evaluate, rules_write) before each launch, in the launch's layout."""
+    if case == "bouzidi":
+        p, _ = cases.bouzidi(NS, d, dtype)
+    else:
+        p, _ = cases.open_channel_case(NS, d, dtype=dtype)
+    start = OracleSolver(p)
+    start.initialize(*cases.random_state(p, seed=1, u_scale=0.03))
+    f0 = start.populations()
+    ref = ref_kernels.RefSolver(p, variant)
+    assert ref.rule_passes
+    ref.set_populations(f0)
+    ours = lbm.make_solver(p, backend="cuda-aa" if variant == "aa" else "cuda-naive")
+    ours.set_populations(f0)
+    ref.advance(cases.EQUIVALENCE_STEPS)
+    ours.run(cases.EQUIVALENCE_STEPS)
+    fluid = p.fluid
+    diff = float(np.abs(ref.populations()[:, fluid] - ours.populations()[:, fluid]).max())
+    assert diff < ABS[dtype], diff
 
 
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
