@@ -31,7 +31,7 @@ def reference_namespace(src: str):
     from lbm.geometry import circle, sphere, voxelize, wall_links
     from lbm.ibm import ImmersedBoundary
     from lbm.lattice import default_lattice
-    from lbm.link_rules import LAYOUTS, LinkRules, bouzidi_rules, compile_affine
+    from lbm.link_rules import LAYOUTS, LinkRules, bouzidi_rules, compile_affine, compile_rules
     from lbm.open_boundaries import open_channel
     from lbm.solver import SimulationDiverged
 
@@ -39,7 +39,7 @@ def reference_namespace(src: str):
         SimulationParams=SimulationParams, make_solver=make_solver, channel_walls=channel_walls,
         cavity_walls=cavity_walls, circle=circle, sphere=sphere, voxelize=voxelize,
         wall_links=wall_links, ImmersedBoundary=ImmersedBoundary, default_lattice=default_lattice,
-        LinkRules=LinkRules, bouzidi_rules=bouzidi_rules, compile_affine=compile_affine,
+        LinkRules=LinkRules, bouzidi_rules=bouzidi_rules, compile_affine=compile_affine, compile_rules=compile_rules,
         open_channel=open_channel, ForceProbe=ForceProbe, LAYOUTS=LAYOUTS,
         SimulationDiverged=SimulationDiverged,
     )
@@ -122,6 +122,20 @@ def main(src: str) -> None:
         p, inflow = cases.open_channel_case(ns, d)
         s = run(ns, p, cases.random_state(p, seed=1, u_scale=0.03), steps)
         save(f"zouhe{d}d_float64", steps=steps, solid=p.solid, **rules_arrays("rule_", p.link_rules), **outputs(s, d))
+
+    # Link rules compiled to the pre-pass slots of every layout (the reference's
+    # compile_rules), for the cases the GPU checker runs against the reference's
+    # own rule pre-pass kernels
+    compiled = {}
+    for d in (2, 3):
+        for name, (p, _) in (("bouzidi", cases.bouzidi(ns, d, "float64")),
+                             ("zouhe", cases.open_channel_case(ns, d))):
+            for layout in ("pull", "aa_odd", "aa_even"):
+                c = ns.compile_rules(p.lattice, p.link_rules, layout, p.solid, p.wall_velocity)
+                key = f"{name}{d}d_{layout}_"
+                compiled |= {key + "target": np.asarray(c.target), key + "slots": np.asarray(c.values.slots),
+                             key + "coeff": np.asarray(c.values.coeff), key + "const": np.asarray(c.values.constant)}
+    save("compiled_rules", **compiled)
 
     # Configuration geometries: rule builders only (no run)
     p, links, _ = cases.cylinder_channel(ns, "bouzidi")

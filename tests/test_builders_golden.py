@@ -154,3 +154,38 @@ def test_rules_validation():
         lbm.SimulationParams(nx=33, ny=21, tau=0.7, solid=solid, wall_velocity=moving, link_rules=rules)
     with pytest.raises(ValueError, match="more than one"):
         lbm.LinkRules(np.array([5, 5]), np.array([3, 3]), lbm.AffineSet.from_lists([[(1, 0, 1.0)], [(1, 0, 1.0)]]))
+
+
+def _compiled_map(target, slots, coeff, const):
+    """{target slot: (constant, {term slot: coefficient})}, zero terms dropped, any rule order."""
+    out = {}
+    for t, s, c, k in zip(target, slots, coeff, const, strict=True):
+        terms = {}
+        for slot, a in zip(s, c, strict=True):
+            if a != 0.0:
+                terms[int(slot)] = terms.get(int(slot), 0.0) + float(a)
+        out[int(t)] = (float(k), terms)
+    return out
+
+
+@pytest.mark.parametrize("layout", ["pull", "aa_odd", "aa_even"])
+@pytest.mark.parametrize("case", ["bouzidi", "zouhe"])
+@pytest.mark.parametrize("d", [2, 3])
+def test_rules_compile_to_the_reference_prepass_slots(d, case, layout):
+    """compile_rules (the pre-pass form that the GPU checker feeds to the reference's own
+    rule kernels) gives the reference's targets, term slots, coefficients and constants."""
+    from lbm_b200.link_rules import compile_rules
+
+    ref = golden("compiled_rules")
+    key = f"{case}{d}d_{layout}_"
+    p, _ = cases.bouzidi(NS, d, "float64") if case == "bouzidi" else cases.open_channel_case(NS, d)
+    c = compile_rules(p.lattice, p.link_rules, layout, p.solid, p.wall_velocity)
+    ours = _compiled_map(c.target, c.values.slots, c.values.coeff, c.values.constant)
+    theirs = _compiled_map(ref[key + "target"], ref[key + "slots"], ref[key + "coeff"], ref[key + "const"])
+    assert ours.keys() == theirs.keys()
+    for t, (k, terms) in theirs.items():
+        k2, terms2 = ours[t]
+        assert abs(k - k2) <= 1e-15, (t, k, k2)
+        assert terms.keys() == terms2.keys(), t
+        for slot, a in terms.items():
+            assert abs(a - terms2[slot]) <= 1e-15, (t, slot)
