@@ -200,10 +200,11 @@ class BatchedSolver:
             shape = tuple(self.params[i].shape)
             n = g.nx * g.ny * g.nz
             rho_t = torch.zeros(g.qstride, dtype=torch.float64, device=self.device)
-            rho_t[:n] = torch.as_tensor(np.broadcast_to(np.asarray(rho, dtype=np.float64), shape).reshape(-1), device=self.device)
+            # torch.tensor copies: a broadcast (read-only) view is fine
+            rho_t[:n] = torch.tensor(np.broadcast_to(np.asarray(rho, dtype=np.float64), shape).reshape(-1), device=self.device)
             u_t = torch.zeros((d, g.qstride), dtype=torch.float64, device=self.device)
             for a, c in enumerate((ux, uy, uz)[:d]):
-                u_t[a, :n] = torch.as_tensor(np.broadcast_to(np.asarray(c, dtype=np.float64), shape).reshape(-1), device=self.device)
+                u_t[a, :n] = torch.tensor(np.broadcast_to(np.asarray(c, dtype=np.float64), shape).reshape(-1), device=self.device)
             ph = self._physics(i)
             N.call("lbm_init_equilibrium", N.C.byref(g), N.C.byref(ph), N.ptr(rho_t), N.ptr(u_t), N.LAYOUT_PULL,
                    N.ptr(self._slice(self._f, i)), stream)
