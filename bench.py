@@ -132,7 +132,33 @@ def run_reference(args, rank):
         "note": "NumPy restatement of the reference ReferenceSolver (the reference is pure Python and is "
                 "not installed on the GPU host); NumPy element-wise work is single-threaded",
     }
+    gpu = reference_gpu_kernels(args)
+    if gpu is not None:
+        line["reference_gpu_kernels"] = gpu
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_kernels(args):
+    """For information beside the CPU value: the reference's own CUDA kernels (compiled unmodified
+    for sm_100a into oracle/_ref) on the same duct, float32, timed with CUDA events; None when the
+    libraries or a GPU are missing."""
+    try:
+        import torch
+
+        from oracle import ref_kernels
+
+        if not torch.cuda.is_available() or not ref_kernels.available():
+            return None
+        import lbm_b200 as lbm
+
+        torch.cuda.set_device(0)
+        params = duct_params(lbm, args.n, storage="float32")
+        out = {v: round(ref_kernels.time_reference(params, v, 100), 1) for v in ("naive", "aa")}
+        out |= {"unit": "MLUPS", "workload": f"D3Q19 duct {args.n}^3 float32, 100 steps after 100 untimed",
+                "kernels": "stream_collide_naive; aa_odd + aa_even (reference src/lbm/backends/kernels)"}
+        return out
+    except Exception as exc:  # noqa: BLE001 -- informational only; the CPU value stands
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
 
 
 def workload_config(args):

@@ -314,6 +314,27 @@ class RefSolver:
         return f.cpu().numpy()
 
 
+def time_reference(params, variant: str, steps: int) -> float:
+    """MLUPS of the reference's kernels alone on `params` (from the rest state), CUDA events;
+    the same number of steps runs untimed first."""
+    import numpy as np
+    import torch
+
+    ref = RefSolver(params, variant)
+    ref.set_populations(torch.zeros((params.lattice.q, *params.shape), dtype=ref.t_real))
+    ref.advance(steps)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    ref.advance(steps)
+    b.record()
+    b.synchronize()
+    mlups = int(np.prod(params.shape)) * steps / a.elapsed_time(b) / 1e3
+    del ref
+    torch.cuda.empty_cache()
+    return mlups
+
+
 def _time_pair(lbm, torch, params, steps: int, variant: str):
     """MLUPS of the reference kernel and of this repository's step on the same grid (CUDA events);
     each side first runs the same number of steps untimed (so this repository's CUDA graphs for
