@@ -33,7 +33,9 @@ from .params import COMPUTE_DTYPE
 
 DEFAULT_CHECK_EVERY = 500
 DEFAULT_BLOCK = (32, 4)
-BACKENDS = ("cuda", "cuda-naive", "cuda-aa")
+BACKENDS = ("cuda", "cuda-naive", "cuda-tiled", "cuda-aa")
+"""``cuda-tiled`` keeps the reference's 2D-only backend name working: this build's pull
+step (its shared-memory staging is the TMA kernel for 16-bit storage)."""
 VARIANTS = ("pull", "aa")
 
 
@@ -75,6 +77,8 @@ def make_solver(params, backend: str = "cuda", **options) -> CudaSolver:
     """
     if backend not in BACKENDS:
         raise ValueError(f"unknown backend {backend!r}; choose from {BACKENDS}")
+    if backend == "cuda-tiled" and params.d != 2:  # reference cuda_solver.py:56-62
+        raise ValueError(f"CUDA variant 'tiled' is 2D only; use 'naive' or 'aa' for a {params.d}D grid")
     return CudaSolver(params, variant="aa" if backend == "cuda-aa" else "pull", **options)
 
 

@@ -70,7 +70,9 @@ def test_backend_registry_and_errors():
     params = lbm.SimulationParams(nx=8, ny=8, tau=0.8)
     with pytest.raises(ValueError, match="backend"):
         lbm.make_solver(params, backend="opencl")
-    assert lbm.BACKENDS == ("cuda", "cuda-naive", "cuda-aa")
+    assert lbm.BACKENDS == ("cuda", "cuda-naive", "cuda-tiled", "cuda-aa")
+    with pytest.raises(ValueError, match="2D only"):
+        lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, nz=8, tau=0.8), backend="cuda-tiled")
 
 
 def test_solver_without_gpu_raises_backend_unavailable():

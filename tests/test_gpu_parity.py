@@ -333,6 +333,17 @@ def test_pull_and_aa_give_identical_bits(d, dtype):
     np.testing.assert_array_equal(a.populations()[:, p.fluid], b.populations()[:, p.fluid])
 
 
+def test_tiled_backend_name_runs_the_pull_step():
+    """The reference's 2D-only cuda-tiled name: the same bits as cuda-naive."""
+    p = cases.mixed(NS, "float32", "trt", 2)
+    a = lbm.make_solver(p, backend="cuda-tiled")
+    b = lbm.make_solver(p, backend="cuda-naive")
+    for s in (a, b):
+        s.initialize(*cases.random_state(p))
+        s.run(10)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+
+
 @pytest.mark.parametrize("backend", BACKENDS)
 def test_graph_and_eager_launches_agree(backend):
     p = cases.mixed(NS, "float32", "trt", 2)
