@@ -5,9 +5,13 @@ Workload (the configuration the headline metric is quoted on): D3Q19 TRT,
 tau = 0.9, Lambda = 3/16, 256 x 256 x 256 nodes, solid layers at y = 0, 255
 and z = 0, 255, periodic in x, Guo body force Fx = 1e-6, float32 storage.
 One bench "step" is one LBM time step over the whole lattice: one launch of
-the bulk kernel (the duct has no link rules, so no boundary launch), replayed
-from a CUDA graph captured during warm-up. The lattice (2 x 1.27 GB) is ~20x
-the 126 MB L2, so every step streams from HBM; no L2 flush is needed.
+the bulk kernel (the duct has no link rules, so no boundary launch); runs of
+32 steps replay a CUDA graph captured before the warm-up. The lattice
+(2 x 1.27 GB) is ~20x the 126 MB L2, so every step streams from HBM; no L2
+flush is needed. Timing: exactly W warm-up steps, then timed regions of
+exactly K steps (CUDA events between barriers, max over ranks), repeated
+until they span 2 s so that the nvidia-smi clock samples (every 50 ms) see
+the GPU under load; ``ms_per_step`` is the median region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--variant pull|aa]
                     [--storage float32|float16|bfloat16|float64] [--impl reference]
@@ -20,8 +24,10 @@ rho/u (float64), ``run`` of a chunk of time steps, ``macroscopic`` back to the
 host. ``roofline.achieved`` = 152 B per update (2 Q float32, the reference's
 count, benchmarks/bench_mlups.py:9-10) x the nodes of one launch over the
 CUDA-event time per step (one launch per step, so an upper bound on the
-launch duration). ``cpu_baseline`` times the NumPy oracle (a restatement of the reference's
-CPU solver) on a bounded slab of the same duct on this host.
+launch duration). ``cpu_baseline`` times the reference's own CPU solver
+(``ReferenceSolver(params, xp=numpy)``, the unmodified package in
+baseline/_ref; the NumPy oracle port where that is absent) on a bounded slab
+of the same duct on this host; ``--impl reference`` times the same.
 """
 
 from __future__ import annotations
@@ -47,6 +53,8 @@ METRIC = "D3Q19 256\u00b3 MLUPS, %HBM peak: fp32 vs fp16-store at \u22641e-3 u e
 BYTES = {"float32": 4, "float64": 8, "float16": 2, "bfloat16": 2}
 DTYPE_TAG = {"float32": "f32", "float64": "f64", "float16": "f16-store/f32", "bfloat16": "bf16-store/f32"}
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+MIN_TIMED_SECONDS = 2.0
+MIN_REPEATS, MAX_REPEATS = 3, 100000
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -91,35 +99,72 @@ def duct_params(lbm, n, nx=None, nz=None, storage="float32"):
 
 
 # --------------------------------------------------------------------- CPU side
+def duct_slab_solid(n: int, nz: int) -> np.ndarray:
+    solid = np.zeros((nz, n, n), dtype=bool)
+    solid[:, [0, -1], :] = True
+    solid[[0, -1], :, :] = True
+    return solid
+
+
+def _time_steps(step, steps: int, warmup: int, budget: float | None):
+    """Call ``step()`` `warmup` times, then time at least `steps` calls (more, up to 10x, while under
+    `budget` seconds; at least 3): (calls timed, seconds)."""
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps or (budget is not None and time.perf_counter() - t0 < budget and done < 10 * steps):
+        step()
+        done += 1
+        if budget is not None and time.perf_counter() - t0 >= budget and done >= 3:
+            break
+    return done, time.perf_counter() - t0
+
+
 def oracle_mlups(n: int, nz: int, steps: int, warmup: int, budget: float | None = None):
     """NumPy oracle on an n x n x nz slab of the duct: (MLUPS, steps timed, seconds)."""
     import lbm_b200 as lbm
     from oracle import OracleSolver
 
-    p = duct_params(lbm, n, nz=nz)
-    s = OracleSolver(p)
-    for _ in range(warmup):
-        s.step()
-    t0 = time.perf_counter()
-    done = 0
-    while done < steps or (budget is not None and time.perf_counter() - t0 < budget and done < 10 * steps):
-        s.step()
-        done += 1
-        if budget is not None and time.perf_counter() - t0 >= budget and done >= 3:
-            break
-    dt = time.perf_counter() - t0
+    s = OracleSolver(duct_params(lbm, n, nz=nz))
+    done, dt = _time_steps(s.step, steps, warmup, budget)
     return n * n * nz * done / dt / 1e6, done, dt
 
 
+def cpu_reference_mlups(n: int, nz: int, steps: int, warmup: int, budget: float | None = None):
+    """The reference's own CPU solver, ``ReferenceSolver(params, xp=numpy)`` from the unmodified
+    package in baseline/_ref (``make_solver(params, backend="numpy")``), one ``_advance(1)`` per step,
+    on an n x n x nz slab of the duct: (MLUPS, steps timed, seconds, kind). Without baseline/_ref
+    the NumPy oracle port stands in (kind "port")."""
+    from oracle import reference_package
+
+    ref = reference_package.modules()
+    if ref is None:
+        mlups, done, dt = oracle_mlups(n, nz, steps, warmup, budget)
+        return mlups, done, dt, "port"
+    params = ref.params.SimulationParams(nx=n, ny=n, nz=nz, tau=0.9, collision="trt", force=(1e-6, 0.0, 0.0),
+                                         solid=duct_slab_solid(n, nz), dtype="float32")
+    s = ref.backends.make_solver(params, backend="numpy")
+    s.initialize()
+    done, dt = _time_steps(lambda: s._advance(1), steps, warmup, budget)
+    return n * n * nz * done / dt / 1e6, done, dt, "reference"
+
+
+CPU_KIND_NOTE = {
+    "reference": "the unmodified reference ReferenceSolver(params, xp=numpy) from baseline/_ref",
+    "port": "the NumPy oracle port of the reference ReferenceSolver (baseline/_ref not installed)",
+}
+
+
 def run_reference(args, rank):
-    """Reference arm: the NumPy oracle port of the reference CPU solver, rank 0 only."""
+    """Reference arm: the reference's own CPU solver (NumPy), rank 0 only."""
     if rank != 0:
         return
     n = args.n
     # size the slab so that K steps take about a minute; a larger K is cut off at a 60 s budget
     per_node = 1.0 / 1.4e6
     nz = int(min(16, max(3, round(60.0 / (max(args.steps, 1) * n * n * per_node)))))
-    mlups, done, dt = oracle_mlups(n, nz, args.steps, min(args.warmup, 3), budget=60.0)
+    mlups, done, dt, kind = cpu_reference_mlups(n, nz, args.steps, min(args.warmup, 3), budget=60.0)
     sample = (f"{n}x{n}x{nz} slab of the duct (same walls, force, tau), {done} steps timed ({args.steps} asked; "
               f"up to 10x as many while under a 60 s budget) after {min(args.warmup, 3)} warm-up")
     line = {
@@ -127,10 +172,10 @@ def run_reference(args, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / done, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args),
-        "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": 1, "kind": kind, "sample": sample},
         "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "NumPy restatement of the reference ReferenceSolver (the reference is pure Python and is "
-                "not installed on the GPU host); NumPy element-wise work is single-threaded",
+        "note": f"{CPU_KIND_NOTE[kind]}; NumPy element-wise work runs on one thread "
+                f"(host has {os.cpu_count()} cores)",
     }
     gpu = reference_gpu_kernels(args)
     if gpu is not None:
@@ -175,19 +220,21 @@ def workload_config(args):
 
 # --------------------------------------------------------------------- GPU side
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons sampled every `interval_ms` while running."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_uuid: str | None):
+    def __init__(self, device_uuid: str | None, interval_ms: int = 50):
         self.uuid = device_uuid
+        self.interval_ms = int(interval_ms)
         self.proc = None
         self.lines: list[str] = []
 
     def __enter__(self):
-        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms",
+               str(self.interval_ms)]
         if self.uuid:
             cmd.insert(1, f"--id={self.uuid}")
         try:
@@ -547,8 +594,7 @@ def run_ours(args, rank, world, local_rank):
     block = tuple(int(v) for v in args.block.split("x"))
     solver = lbm.make_solver(params, backend=backend, launch=args.launch, block=block)
     steps = args.steps + (args.steps % solver.step_multiple)
-    warm = max(args.warmup, 3)
-    warm += warm % solver.step_multiple
+    warm = args.warmup + (args.warmup % solver.step_multiple)
 
     def barrier():
         torch.cuda.synchronize()
@@ -556,8 +602,11 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     stream = torch.cuda.current_stream()
-    # warm-up also captures the CUDA graph the timed run replays
-    warm = max(warm, solver.GRAPH_CHUNK)
+    # The CUDA graph that chunks of GRAPH_CHUNK steps replay is captured first:
+    # capture records the launches without running them, so the warm-up below
+    # is exactly the requested number of steps.
+    if solver.use_graph and steps >= solver.GRAPH_CHUNK:
+        solver._graph(solver.GRAPH_CHUNK)
     solver._advance(warm)
     barrier()
     uuid = None
@@ -566,17 +615,29 @@ def run_ours(args, rank, world, local_rank):
     except Exception:  # noqa: BLE001
         uuid = None
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(uuid) as clocks:
+
+    def timed_steps() -> float:
+        """One timed region of exactly `steps` steps between barriers; the slowest rank's milliseconds."""
         barrier()
         start.record(stream)
         solver._advance(steps)
         stop.record(stream)
         stop.synchronize()
         barrier()
-    ms = start.elapsed_time(stop)
-    solver.time_step += warm + steps
+        return max_over_ranks(start.elapsed_time(stop), world, device)
+
+    # The timed region (exactly `steps` steps) is repeated until the repeats
+    # span at least MIN_TIMED_SECONDS, so that the clock sampler sees the GPU
+    # under load; the repeat count follows from the first repeat's max over
+    # ranks, the same on every rank. `ms_per_step` is the median repeat.
+    with ClockSampler(uuid, interval_ms=50) as clocks:
+        times = [timed_steps()]
+        repeats = int(min(MAX_REPEATS, max(MIN_REPEATS, math.ceil(MIN_TIMED_SECONDS * 1e3 / max(times[0], 1e-3)))))
+        for _ in range(repeats - 1):
+            times.append(timed_steps())
+    solver.time_step += warm + steps * len(times)
     solver._check_health()
-    ms = max_over_ranks(ms, world, device)
+    ms = statistics.median(times)
     mlups = whole_job_mlups(nodes, steps, ms, world)
     ms_step = ms / steps
 
@@ -618,6 +679,10 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": world, "steps": steps,
         "warmup": warm, "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak",
+        "timing": {"repeats": len(times), "region_steps": steps, "stat": "median over repeats of the timed region",
+                   "ms_per_step_min": round(min(times) / steps, 5), "ms_per_step_max": round(max(times) / steps, 5),
+                   "seconds_timed": round(sum(times) / 1e3, 3), "launches_per_region": steps,
+                   "launches_all_repeats": steps * len(times)},
         "vs_baseline": None, "dtype": DTYPE_TAG[args.storage], "data": "synthetic (analytic duct set-up, fluid at rest)",
         "config": workload_config(args),
         "roofline": {"bound": "hbm", "kernel": step_kernel_name(args),
@@ -651,9 +716,9 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.empty_cache()
         line["adjoint"] = adjoint_study(lbm, torch)
     if not args.no_cpu_baseline and world == 1:
-        mlups_cpu, done, dt = oracle_mlups(n, 8, 3, 1, budget=args.cpu_seconds)
-        line["cpu_baseline"] = {"value": round(mlups_cpu, 4), "unit": "MLUPS", "cores": 1, "kind": "port",
-                                "sample": f"{n}x{n}x8 slab of the duct, {done} steps in {dt:.1f} s (NumPy oracle, "
+        mlups_cpu, done, dt, kind = cpu_reference_mlups(n, 8, 3, 1, budget=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(mlups_cpu, 4), "unit": "MLUPS", "cores": 1, "kind": kind,
+                                "sample": f"{n}x{n}x8 slab of the duct, {done} steps in {dt:.1f} s ({CPU_KIND_NOTE[kind]}; "
                                           f"single-threaded element-wise; host has {os.cpu_count()} cores)"}
     print(json.dumps(line), flush=True)
 

@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 3
+ABI_VERSION = 5
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -29,6 +29,7 @@ LAYOUT_PULL, LAYOUT_AA_ODD, LAYOUT_AA_EVEN = 0, 1, 2
 KIND_SOLID, KIND_SPECIAL, KIND_NEAR, KIND_EDGE = 1, 2, 4, 8
 LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY = 0, 1, 2
 LAUNCH_MODES = (LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY)
+TMA_WAIT_NONE = 0xFFFFFFFF
 
 STORAGE_CODE = {"float32": LBM_F32, "float64": LBM_F64, "float16": LBM_F16, "bfloat16": LBM_BF16}
 LATTICE_CODE = {"D2Q9": LBM_D2Q9, "D3Q19": LBM_D3Q19}
@@ -66,8 +67,12 @@ class Special(C.Structure):
     ]
 
 
+class Health(C.Structure):
+    _fields_ = [("words", vp), ("partial", vp), ("n_partial", i64)]
+
+
 class Launch(C.Structure):
-    _fields_ = [("tile_x", i32), ("tile_y", i32), ("mode", i32)]
+    _fields_ = [("tile_x", i32), ("tile_y", i32), ("mode", i32), ("tma_wait_limit", u32), ("health", C.POINTER(Health))]
 
 
 class Ibm(C.Structure):
@@ -116,6 +121,7 @@ _SIGNATURES = {
     "lbm_pack": [P(Grid), vp, i32, vp, vp],
     "lbm_macroscopic": [P(Grid), P(Physics), vp, vp, i32, vp, vp, i32, vp, vp, vp],
     "lbm_health_reset": [vp, vp],
+    "lbm_health_finish": [P(Health), vp, vp],
     "lbm_health": [P(Grid), vp, vp, vp, vp],
     "lbm_affine_gather": [i32, vp, vp, vp, vp, i64, i32, vp, vp],
     "lbm_affine_reduce": [i32, vp, vp, vp, vp, vp, i64, i32, i32, vp, vp, vp, vp],
@@ -128,7 +134,7 @@ _SIGNATURES = {
     "lbm_ibm_adjoint_moments": [P(Grid), P(Ibm), vp, vp, vp],
     "lbm_kernel_resources": [i32, i32, i32, vp],
 }
-EXPORTED = (*_SIGNATURES, "lbm_last_cuda_error", "lbm_abi_version")
+EXPORTED = (*_SIGNATURES, "lbm_health_partials", "lbm_last_cuda_error", "lbm_abi_version")
 
 _lib = None
 
@@ -149,6 +155,8 @@ def load(path: Path | None = None):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = C.c_int
+    lib.lbm_health_partials.argtypes = [P(Grid), P(Special), P(Launch)]
+    lib.lbm_health_partials.restype = i64
     lib.lbm_last_cuda_error.restype = C.c_char_p
     lib.lbm_last_cuda_error.argtypes = []
     lib.lbm_abi_version.restype = i32

@@ -421,7 +421,7 @@ class AdjointRun:
                 if free[rid] is not None:
                     rec_stream.wait_event(free[rid])
                 rings[rid][0].copy_(self._checkpoints[start])
-                if n == K:
+                if n == K and K > 1:  # (K = 1: the checkpoint alone, nothing to recompute or capture)
                     key = ("recompute", rid)
                     if key not in graphs:
                         graphs[key] = self._capture(lambda: recompute(rings[rid], K))

@@ -79,6 +79,7 @@ def tune_step(solver, tiles=TILES, steps: int = 20) -> dict:
     tx, ty = best["block"]
     solver._launches = {m: N.Launch(tx, ty, m) for m in N.LAUNCH_MODES}
     solver.block = (tx, ty)
+    solver._setup_checked_launches()  # the checked step's partial sums follow the tile
     solver._graphs.clear()
     return best
 

@@ -41,6 +41,20 @@ static bool special_valid(const lbm_special_t* sp, bool aa)
     return true;
 }
 
+// Partial slots of a checked step: the bulk grid's blocks, then (split) the
+// boundary launch's or (fused) the extra planes'.
+static int64_t health_partials(const lbm_grid_t* g, const lbm_special_t* sp, int tx, int ty, int mode)
+{
+    const int64_t gx = (g->nx + tx - 1) / tx, gy = (g->ny + ty - 1) / ty;
+    const int64_t ns = sp ? sp->n_special : 0;
+    if (mode == LBM_LAUNCH_FUSED) {
+        const int64_t per_plane = gx * gy * tx * ty;
+        const int64_t extra = ns > 0 ? (ns + per_plane - 1) / per_plane : 0;
+        return gx * gy * (g->nz + extra);
+    }
+    return gx * gy * g->nz + (ns + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS;
+}
+
 static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
                      const lbm_launch_t* launch, const uint8_t* kind, const void* src, void* dst, int& tx, int& ty,
                      int& mode)
@@ -71,10 +85,21 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
     if (half && !p->round_seed) return LBM_ERR_INVALID;
     a.seed = half ? p->round_seed : nullptr;
     a.parity = 0;
+    a.health_words = nullptr;
+    a.health_partial = nullptr;
+    a.health_slot0 = 0;
+    a.wait_limit = WAIT_LIMIT_DEFAULT;
+    if (launch && launch->tma_wait_limit) a.wait_limit = launch->tma_wait_limit == LBM_TMA_WAIT_NONE ? 0u : launch->tma_wait_limit;
     if (sp)
         a.sp = *sp;
     else
         memset(&a.sp, 0, sizeof(a.sp));
+    if (launch && launch->health) {
+        const lbm_health_t* h = launch->health;
+        if (!h->words || !h->partial || h->n_partial != health_partials(g, sp, tx, ty, mode)) return LBM_ERR_INVALID;
+        a.health_words = h->words;
+        a.health_partial = h->partial;
+    }
     // collision constants, computed once per launch
     a.guo_const = true;
     if (g->lattice == LBM_D2Q9) {
@@ -125,6 +150,15 @@ extern "C" int lbm_step_aa(const lbm_grid_t* g, const lbm_physics_t* p, const lb
     return record(run());
 }
 
+extern "C" int64_t lbm_health_partials(const lbm_grid_t* g, const lbm_special_t* sp, const lbm_launch_t* launch)
+{
+    if (!grid_valid(g) || !launch || !special_valid(sp, false)) return LBM_ERR_INVALID;
+    const int tx = launch->tile_x, ty = launch->tile_y, mode = launch->mode;
+    if (tx <= 0 || ty <= 0 || tx % 32 != 0 || tx * ty > 256) return LBM_ERR_INVALID;
+    if (mode < LBM_LAUNCH_FUSED || mode > LBM_LAUNCH_BOUNDARY) return LBM_ERR_INVALID;
+    return health_partials(g, sp, tx, ty, mode);
+}
+
 template <class L, int ST>
 static int resources_dispatch(int which, int32_t* out4)
 {
@@ -140,4 +174,4 @@ extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t wh
 
 extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
 
-extern "C" int32_t lbm_abi_version(void) { return 3; }
+extern "C" int32_t lbm_abi_version(void) { return 5; }

@@ -246,6 +246,23 @@ __global__ void health_kernel(const lbm_grid_t g, const uint8_t* __restrict__ ki
     if (any_nf && (threadIdx.x & 31) == 0) atomicMax((unsigned long long*)(out + 1), 1ull);
 }
 
+// Sum of the checked step's per-block partials in a fixed order: 256 threads
+// each add a strided subset in index order, then a fixed tree.
+__global__ void __launch_bounds__(256) health_finish_kernel(const double* __restrict__ partial, int64_t n,
+                                                            double* __restrict__ out)
+{
+    __shared__ double sums[256];
+    double s = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += 256) s += partial[i];
+    sums[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sums[threadIdx.x] += sums[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sums[0];
+}
+
 template <class L, int ST>
 int health(const lbm_grid_t& g, const uint8_t* kind, const void* f, int64_t* out, cudaStream_t s)
 {
@@ -401,6 +418,13 @@ extern "C" int lbm_health_reset(int64_t* out, lbm_stream_t stream)
     return launch_status();
 }
 
+extern "C" int lbm_health_finish(const lbm_health_t* h, double* delta_mass, lbm_stream_t stream)
+{
+    if (!h || !h->partial || h->n_partial <= 0 || !delta_mass) return LBM_ERR_INVALID;
+    health_finish_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(h->partial, h->n_partial, delta_mass);
+    return launch_status();
+}
+
 extern "C" int lbm_health(const lbm_grid_t* g, const uint8_t* kind, const void* f, int64_t* out, lbm_stream_t stream)
 {
     if (!grid_ok(g) || !kind || !f || !out) return LBM_ERR_INVALID;
@@ -472,22 +496,29 @@ constexpr int64_t kStaticReduceBlocks = (LBM_AFFINE_REDUCE_STATIC_MAX_ROWS + 255
 constexpr int64_t kStaticReduceHead = 32;  // doubles: 256 bytes
 static __device__ __align__(256) double g_reduce_scratch[kStaticReduceHead + kStaticReduceBlocks * 3];
 
-// Device address of g_reduce_scratch, looked up once per device (with that
-// device current) and cached; the lookup may load this library's device code.
+// Device address of g_reduce_scratch, looked up once per device context (with
+// that device current) and cached; the lookup may load this library's device
+// code. The cache is keyed by the context's id: after cudaDeviceReset the
+// device's new context holds a new copy of the array, whose address is looked
+// up again on the first call made in it.
 constexpr int kMaxDevices = 64;
 static std::mutex g_scratch_mutex;
 static double* g_scratch_ptr[kMaxDevices];
+static unsigned long long g_scratch_ctx[kMaxDevices];
 
 static int static_reduce_scratch(double** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return LBM_ERR_LAUNCH;
     if (dev < 0 || dev >= kMaxDevices) return LBM_ERR_UNSUPPORTED;
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (g_scratch_ptr[dev] == nullptr) {
+    if (g_scratch_ptr[dev] == nullptr || ctx == 0 || ctx != g_scratch_ctx[dev]) {
         void* p = nullptr;
+        // (creates the device's context if this thread has none yet)
         if (cudaGetSymbolAddress(&p, g_reduce_scratch) != cudaSuccess || p == nullptr) return LBM_ERR_LAUNCH;
         g_scratch_ptr[dev] = static_cast<double*>(p);
+        g_scratch_ctx[dev] = current_context_id();
     }
     *out = g_scratch_ptr[dev];
     return LBM_OK;

@@ -314,6 +314,12 @@ __host__ __device__ __forceinline__ double r_mul(double a, double b)
 
 constexpr int QMAX = 19;
 
+// Threads per block of the boundary-warp launches (LBM_LAUNCH_BOUNDARY).
+constexpr int BOUNDARY_THREADS = 32;
+
+// Default bound, in polls, of every wait of a TMA-staged kernel on an mbarrier.
+constexpr uint32_t WAIT_LIMIT_DEFAULT = 1u << 22;
+
 // Node-independent collision constants of one launch (see above).
 template <class R>
 struct Relax {
@@ -530,6 +536,11 @@ struct StepArgs {
     // reads seed[parity] and its bulk part writes seed[parity ^ 1] = +1.
     uint32_t* seed;
     int parity;
+    uint32_t wait_limit;  // polls of a TMA-staged block's wait for a tile (lbm_launch_t.tma_wait_limit)
+    // Health and mass epilogue of a checked step (lbm_launch_t.health; null words: off).
+    int64_t* health_words;    // [0] first bad pitched node (atomicMin), [1] 1 if non-finite (atomicMax)
+    double* health_partial;   // one float64 sum per block of the launch
+    int64_t health_slot0;     // partial slot of this launch's first block
     lbm_special_t sp;
     bool guo_const;    // rf/rd hold kC, kG of the uniform force (else computed per node)
     Relax<float> rf;   // collision constants (float arithmetic)
@@ -543,6 +554,57 @@ struct StepArgs {
     }
 };
 
+// ---------------------------------------------------------------- health epilogue
+// On the step that ends a chunk of the run loop, the step kernels also check
+// the state they store (reference Solver._check_health, src/lbm/solver.py:162-172):
+// per updated fluid node drho = sum_i f~*_i of the stored (rounded) values in
+// direction order, bad if non-finite or drho <= -1; and they sum f~* in
+// float64 (the mass minus the fluid node count). Each thread accumulates the
+// nodes it updates; health_block then folds the block into one partial sum
+// (warp shuffles, then the warps in order: a fixed order) and the rare bad
+// nodes into the two status words with atomics.
+struct NodeHealth {
+    double dm = 0.0;               // sum of stored f~* of this thread's nodes
+    long long bad = 0x7fffffffffffffffLL;  // smallest bad pitched node
+    bool nonfinite = false;
+};
+
+template <class L, class R>
+__device__ __forceinline__ void health_node(NodeHealth& hl, int64_t nd, const R (&v)[L::Q])
+{
+    R drho = v[0];
+    double dm = (double)v[0];
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        drho = v_add(drho, v[i]);
+        dm += (double)v[i];
+    }
+    hl.dm += dm;
+    const bool nf = !isfinite(drho);
+    if (nf || drho <= R(-1)) hl.bad = nd < hl.bad ? nd : hl.bad;
+    hl.nonfinite |= nf;
+}
+
+// Every thread of the block calls it once (blocks are whole warps).
+__device__ __forceinline__ void health_block(const StepArgs& a, const NodeHealth& hl, int64_t block)
+{
+    __shared__ double warp_dm[32];
+    if (hl.bad != 0x7fffffffffffffffLL) atomicMin((unsigned long long*)a.health_words, (unsigned long long)hl.bad);
+    if (hl.nonfinite) atomicMax((unsigned long long*)(a.health_words + 1), 1ull);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    double x = hl.dm;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if ((tid & 31) == 0) warp_dm[tid >> 5] = x;
+    __syncthreads();
+    if (tid == 0) {
+        double sum = 0.0;
+        const int warps = (int)((blockDim.x * blockDim.y + 31) >> 5);
+        for (int w = 0; w < warps; ++w) sum += warp_dm[w];
+        a.health_partial[a.health_slot0 + block] = sum;
+    }
+}
+
 // The bulk (or fused) launch of a step advances the step counter: one thread
 // writes the other slot, which no thread of this step reads.
 __device__ __forceinline__ void advance_seed(const StepArgs& a)
@@ -550,6 +612,37 @@ __device__ __forceinline__ void advance_seed(const StepArgs& a)
     if (a.seed != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
         threadIdx.y == 0)
         a.seed[a.parity ^ 1] = a.seed[a.parity] + 1u;
+}
+
+// ---------------------------------------------------------------- host
+// Unique id of the calling thread's current CUDA context (cuCtxGetId, which
+// never hands the same id to two contexts of one process), or 0 if there is
+// no current context or the driver cannot say. Per-device state that the
+// library caches -- a device symbol's address, a kernel attribute -- belongs
+// to one context: after cudaDeviceReset the device gets a new context, the
+// library's device code is loaded again and the cached state is stale, so
+// such caches are keyed by this id as well as by the device number.
+inline unsigned long long current_context_id()
+{
+    using GetCurrentFn = int (*)(void**);
+    using GetIdFn = int (*)(void*, unsigned long long*);
+    auto entry = [](const char* name) -> void* {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    };
+    static GetCurrentFn get_current = reinterpret_cast<GetCurrentFn>(entry("cuCtxGetCurrent"));
+    static GetIdFn get_id = reinterpret_cast<GetIdFn>(entry("cuCtxGetId"));
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current == nullptr || get_id == nullptr || get_current(&ctx) != 0 || ctx == nullptr) return 0;
+    if (get_id(ctx, &id) != 0) return 0;
+    return id;
 }
 
 }  // namespace lbm

@@ -163,12 +163,27 @@ struct StepKernel {
         }
     }
 
+    // Health epilogue of a checked step (pull and AA even: the node's stored
+    // values are its post-collision populations): the values as stored,
+    // rounded like the stores for 16-bit formats.
+    __device__ static __forceinline__ void stored_health(const R (&f)[Q], uint32_t h, bool hi, int64_t nd,
+                                                         NodeHealth& hl)
+    {
+        static_assert(VAR != LBM_AA_ODD, "the odd AA half does not store a node's populations at the node");
+        R v[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) v[i] = S::STOCHASTIC ? S::round_sr(f[i], h, i, hi) : f[i];
+        health_node<L, R>(hl, nd, v);
+    }
+
     // Interior fluid node (kind 0: no solid neighbour, not on a face of the
     // box, no rule or local force). Every source and destination offset is
     // the same for all threads (-c_i . strides), so the compiler keeps them in
     // uniform registers and each access is [thread pointer + uniform offset].
     // All Q loads are independent and issued back to back.
-    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd, int64_t pair, bool hi)
+    template <bool H = false>
+    __device__ static __forceinline__ void interior(const StepArgs& a, int64_t nd, int64_t pair, bool hi,
+                                                    NodeHealth* hl = nullptr)
     {
         const int64_t qs = a.qstride;
         const int64_t py = a.pitch;
@@ -194,6 +209,7 @@ struct StepKernel {
         }
         collide_node<L, R>(f, a.template relax<R>(), a.guo_const && a.force_field == nullptr, Fx, Fy, Fz);
         const uint32_t h = S::STOCHASTIC ? sr_pair_hash(pair, a.seed[a.parity]) : 0u;
+        if constexpr (H) stored_health(f, h, hi, nd, *hl);
         T* fd = static_cast<T*>(a.f_dst) + nd;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -210,8 +226,9 @@ struct StepKernel {
     // General path: bb = solid-neighbour mask (bit i: x - c_i is solid, so
     // bit opp(i): x + c_i is solid). No kind byte of a neighbour is loaded,
     // so all Q loads are independent.
-    template <bool SPECIAL>
-    __device__ static __forceinline__ void node(const StepArgs& a, int x, int y, int z, int64_t nd, uint32_t bb, int64_t s)
+    template <bool SPECIAL, bool H = false>
+    __device__ static __forceinline__ void node(const StepArgs& a, int x, int y, int z, int64_t nd, uint32_t bb, int64_t s,
+                                                NodeHealth* hl = nullptr)
     {
         const int64_t qs = a.qstride;
         const R* __restrict__ wall = static_cast<const R*>(a.wall_u);
@@ -293,6 +310,7 @@ struct StepKernel {
         collide_node<L, R>(f, a.template relax<R>(), uniform, Fx, Fy, Fz);
         const uint32_t h = S::STOCHASTIC ? sr_pair_hash(sr_pair(a.nx, a.ny, x, y, z), a.seed[a.parity]) : 0u;
         const bool hi = x & 1;
+        if constexpr (H) stored_health(f, h, hi, nd, *hl);
 
         // ---- store (16-bit formats: stochastic rounding, see sr_pair_hash)
         T* fd = static_cast<T*>(a.f_dst);
@@ -344,26 +362,27 @@ struct StepKernel {
 // path; in any other warp every lane takes the general path (interior lanes
 // with an empty mask), so no warp runs both paths one after the other.
 // Solid nodes are skipped, SPECIAL nodes are left to the boundary warps.
-template <class L, int ST, int VAR>
-__device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z, int64_t nd, bool in)
+template <class L, int ST, int VAR, bool H = false>
+__device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z, int64_t nd, bool in,
+                                          NodeHealth* hl = nullptr)
 {
     using K = StepKernel<L, ST, VAR>;
     const uint8_t k = in ? a.kind[nd] : KIND_SOLID;
     if (__all_sync(0xffffffffu, !in || k == KIND_FLUID)) {
-        if (in) K::interior(a, nd, sr_pair(a.nx, a.ny, x, y, z), x & 1);
+        if (in) K::template interior<H>(a, nd, sr_pair(a.nx, a.ny, x, y, z), x & 1, hl);
     } else if (!(k & (KIND_SOLID | KIND_SPECIAL))) {
-        K::template node<false>(a, x, y, z, nd, a.nbr[nd], -1);
+        K::template node<false, H>(a, x, y, z, nd, a.nbr[nd], -1, hl);
     }
 }
 
 // Bulk: tile (blockIdx.x, blockIdx.y) of plane z; tile_x is a multiple of
 // 32, so every warp lies in one row.
-template <class L, int ST, int VAR>
-__device__ __forceinline__ void bulk_tile(const StepArgs& a, int z)
+template <class L, int ST, int VAR, bool H = false>
+__device__ __forceinline__ void bulk_tile(const StepArgs& a, int z, NodeHealth* hl = nullptr)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    bulk_node<L, ST, VAR>(a, x, y, z, ((int64_t)z * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny);
+    bulk_node<L, ST, VAR, H>(a, x, y, z, ((int64_t)z * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny, hl);
 }
 
 // ---------------------------------------------------------------- vector pull
@@ -589,8 +608,8 @@ template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_B
 
 namespace lbm {
 
-template <class L, int ST, int VAR>
-__device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
+template <class L, int ST, int VAR, bool H = false>
+__device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s, NodeHealth* hl = nullptr)
 {
     if (s >= a.sp.n_special) return;
     const int64_t nd = a.sp.node[s];
@@ -598,7 +617,7 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
     const int x = (int)(nd - row * a.pitch);
     const int y = (int)(row % a.ny);
     const int z = (int)(row / a.ny);
-    StepKernel<L, ST, VAR>::template node<true>(a, x, y, z, nd, a.nbr[nd], s);
+    StepKernel<L, ST, VAR>::template node<true, H>(a, x, y, z, nd, a.nbr[nd], s, hl);
 }
 
 // Bulk-only launches -- this kernel carries almost all of the traffic, so
@@ -608,50 +627,94 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s)
 // registers in float32 arithmetic, four 256-thread blocks per SM cap it at
 // 64 (32 resident warps instead of 24); the float32 pull would take 54, five
 // blocks cap it at 48 (40 warps instead of 36: 38.7 against 37.8 GLUPS).
-template <int ST, int VAR>
+// The checked-step form (H: health epilogue, one step per chunk) keeps the
+// default target.
+template <int ST, int VAR, bool H = false>
 constexpr int bulk_min_blocks()
 {
+    if (H) return 0;
     if (VAR == LBM_AA_ODD && sizeof(typename Storage<ST>::R) == 4) return 4;
     if (VAR == LBM_PULL && ST == LBM_F32) return 5;
     return 0;
 }
 
-template <class L, int ST, int VAR>
-__global__ void __launch_bounds__(256, bulk_min_blocks<ST, VAR>()) lbm_bulk_kernel(const StepArgs a)
+template <class L, int ST, int VAR, bool H = false>
+__global__ void __launch_bounds__(256, bulk_min_blocks<ST, VAR, H>()) lbm_bulk_kernel(const StepArgs a)
 {
     advance_seed(a);
-    bulk_tile<L, ST, VAR>(a, blockIdx.z);
+    if constexpr (H) {
+        NodeHealth hl;
+        bulk_tile<L, ST, VAR, true>(a, blockIdx.z, &hl);
+        health_block(a, hl, ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+    } else {
+        bulk_tile<L, ST, VAR>(a, blockIdx.z);
+    }
 }
 
 // FUSED: grid (ceil(nx/bx), ceil(ny/by), nz + extra), planes z >= nz are
 // boundary warps. BOUNDARY: 1D grid over the list. Up to 255 registers, so
 // the general per-node path never spills.
-template <class L, int ST, int VAR, int MODE>
+template <class L, int ST, int VAR, int MODE, bool H = false>
 __global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
 {
+    NodeHealth hl;
     if (MODE == LBM_LAUNCH_BOUNDARY) {
-        boundary_node<L, ST, VAR>(a, blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+        boundary_node<L, ST, VAR, H>(a, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, &hl);
+        if constexpr (H) health_block(a, hl, blockIdx.x);
         return;
     }
     const int z = blockIdx.z;
     if (z < a.nz) {
         advance_seed(a);
-        bulk_tile<L, ST, VAR>(a, z);
+        bulk_tile<L, ST, VAR, H>(a, z, &hl);
     } else {
         const int64_t b = ((int64_t)(z - a.nz) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        boundary_node<L, ST, VAR>(a, b * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x);
+        boundary_node<L, ST, VAR, H>(a, b * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x, &hl);
     }
+    if constexpr (H) health_block(a, hl, ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
 
-// Boundary launches: one warp per block, so that a few thousand special
-// nodes -- each a long chain of dependent loads (rule terms) -- spread over
-// every SM instead of filling a few (256-thread blocks put an 8,900-node
-// list on 35 of the 148 SMs).
-constexpr int BOUNDARY_THREADS = 32;
+// Boundary launches: one warp per block (BOUNDARY_THREADS), so that a few
+// thousand special nodes -- each a long chain of dependent loads (rule terms)
+// -- spread over every SM instead of filling a few (256-thread blocks put an
+// 8,900-node list on 35 of the 148 SMs).
+
+// A checked step (health epilogue): the one-node bulk kernel, whatever the
+// storage (every bulk kernel gives the same bits), and boundary warps whose
+// per-block sums follow the bulk grid's in the partial array.
+template <class L, int ST, int VAR>
+static int launch_checked(StepArgs a, int mode, int tile_x, int tile_y, cudaStream_t stream)
+{
+    if constexpr (VAR == LBM_AA_ODD) {
+        return LBM_ERR_INVALID;
+    } else {
+        const unsigned gx = (unsigned)((a.nx + tile_x - 1) / tile_x);
+        const unsigned gy = (unsigned)((a.ny + tile_y - 1) / tile_y);
+        if (mode == LBM_LAUNCH_BOUNDARY) {
+            if (a.sp.n_special <= 0) return LBM_OK;
+            a.health_slot0 = (int64_t)gx * gy * a.nz;
+            const int64_t blocks = (a.sp.n_special + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS;
+            lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY, true><<<(unsigned)blocks, BOUNDARY_THREADS, 0, stream>>>(a);
+        } else if (mode == LBM_LAUNCH_BULK) {
+            if (a.nz > 65535) return LBM_ERR_INVALID;
+            a.health_slot0 = 0;
+            lbm_bulk_kernel<L, ST, VAR, true><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+        } else {
+            const int64_t per_plane = (int64_t)gx * gy * tile_x * tile_y;
+            const int64_t extra = a.sp.n_special > 0 ? (a.sp.n_special + per_plane - 1) / per_plane : 0;
+            if (a.nz + extra > 65535) return LBM_ERR_INVALID;
+            a.health_slot0 = 0;
+            lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED, true>
+                <<<dim3(gx, gy, (unsigned)(a.nz + extra)), dim3(tile_x, tile_y), 0, stream>>>(a);
+        }
+        return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+    }
+}
 
 template <class L, int ST, int VAR>
 static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cudaStream_t stream)
 {
+    if (a.health_words != nullptr) return launch_checked<L, ST, VAR>(a, mode, tile_x, tile_y, stream);
     const int threads = tile_x * tile_y;
     const unsigned gx = (unsigned)((a.nx + tile_x - 1) / tile_x);
     const unsigned gy = (unsigned)((a.ny + tile_y - 1) / tile_y);

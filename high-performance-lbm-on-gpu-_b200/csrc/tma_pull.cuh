@@ -24,8 +24,10 @@
 // arithmetic and the rounding are those of the one-node paths.
 //
 // Every wait on an mbarrier is bounded: if a stage has not arrived after
-// TMA_WAIT_LIMIT polls, the block sets status[0] (the caller's status word),
-// waits (bounded) for its other stage and returns.
+// a.wait_limit polls (lbm_launch_t.tma_wait_limit, default
+// WAIT_LIMIT_DEFAULT), the block sets status[0] (the caller's status word),
+// waits for the loads it still has in flight (bounded by the default limit,
+// so that none is outstanding when the block exits) and returns.
 #pragma once
 
 #include <cuda.h>
@@ -42,7 +44,6 @@ constexpr int TMA_ROWS = 2;
 constexpr int TMA_THREADS = 128;
 constexpr int TMA_STAGES = 2;  // tiles in flight per block: TMA_STAGES - 1 ahead of the one computed
 constexpr int TMA_BLOCKS_PER_SM = 5;
-constexpr uint32_t TMA_WAIT_LIMIT = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -71,10 +72,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
     return done != 0u;
 }
 
-// Bounded wait for the phase `phase` of `bar` to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase)
+// Bounded wait (`limit` polls) for the phase `phase` of `bar` to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t limit)
 {
-    for (uint32_t it = 0; it < TMA_WAIT_LIMIT; ++it)
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, phase)) return true;
     return false;
 }
@@ -346,7 +347,7 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
             ty -= tiles_y;
             ++tz;
         }
-        const bool arrived = mbar_wait(&bar[s], (phases >> s) & 1u);
+        const bool arrived = mbar_wait(&bar[s], (phases >> s) & 1u, a.wait_limit);
         if (__syncthreads_or(!arrived)) {
             failed = true;
             break;
@@ -422,7 +423,7 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
         if (tid == 0) atomicOr(status, 1u);
         // wait (bounded) for the loads still in flight into this block's stages
         for (int k = 0; k < TMA_STAGES; ++k)
-            if ((issued >> k) & 1u) mbar_wait(&bar[k], (phases >> k) & 1u);
+            if ((issued >> k) & 1u) mbar_wait(&bar[k], (phases >> k) & 1u, WAIT_LIMIT_DEFAULT);
     }
 }
 
@@ -515,14 +516,17 @@ bool launch_tma(const StepArgs& a, cudaStream_t stream, int* status_out)
         cudaGetLastError();
         return false;
     }
-    static bool configured[64] = {};  // per device: the shared-memory opt-in of this kernel
-    if (!configured[device]) {
+    // per device context: the shared-memory opt-in of this kernel (a new
+    // context after cudaDeviceReset needs it again)
+    static unsigned long long configured[64] = {};
+    const unsigned long long ctx = current_context_id();
+    if (ctx == 0 || configured[device] != ctx) {
         if (cudaFuncSetAttribute(tma_kernel<L, ST, VAR>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(TMA_STAGES * tma_stage_bytes<L>(256) + 8 * TMA_STAGES)) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
-        configured[device] = true;
+        configured[device] = ctx;
     }
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tma_kernel<L, ST, VAR>(), TMA_THREADS, smem) !=

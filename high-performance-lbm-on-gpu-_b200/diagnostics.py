@@ -1,7 +1,7 @@
 """Host snapshot of the macroscopic fields (reference ``src/lbm/diagnostics.py:25-70``).
 
 The CUDA solver computes rho = 1 + sum f~* and rho u = sum c f* - F/2 on the
-device (``csrc/reduce.cu``) and copies the result into this container.
+device (``macro_kernel`` in ``csrc/aux.cu``) and copies the result into this container.
 """
 
 from __future__ import annotations

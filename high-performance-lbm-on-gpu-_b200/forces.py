@@ -7,7 +7,8 @@ For a link from fluid node x into the body (i into the body, j = opp(i))::
 with full populations; f_j(t+1) is the plain bounce-back value or the link's
 rule (reference ``src/lbm/forces.py:47-103``). Shifted storage adds 2 w_i per
 link. ``ForceProbe.evaluate`` hands the functional to the solver, whose CUDA
-path gathers and reduces it in float64 on the device (``csrc/reduce.cu``).
+path gathers and reduces it in float64 on the device (``affine_reduce_kernel`` in
+``csrc/aux.cu``).
 """
 
 from __future__ import annotations

@@ -101,6 +101,11 @@ class Solver(ABC):
     @abstractmethod
     def _check_health(self) -> None: ...
 
+    def _advance_checked(self, steps: int) -> None:
+        """``_advance`` for the run loop: a solver that checks its state inside the last step of
+        the chunk (for ``_check_health`` to read) overrides it."""
+        self._advance(steps)
+
     def run(self, steps: int, *, every: int = 0, callback: Callable | None = None,
             check_every: int = DEFAULT_CHECK_EVERY) -> None:
         """Advance ``steps`` steps (reference ``solver.py:119-160``, same chunking and errors)."""
@@ -117,7 +122,7 @@ class Solver(ABC):
             stop = min(steps, (done // check_every + 1) * check_every)
             if every:
                 stop = min(stop, (done // every + 1) * every)
-            self._advance(stop - done)
+            self._advance_checked(stop - done)
             self.time_step += stop - done
             done = stop
             self._check_health()
@@ -277,10 +282,19 @@ class CudaSolver(Solver):
         if force_field is not None:
             self._force_field = self._upload_field(np.asarray(force_field, dtype=np.float64).reshape(d, *shape))
         self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field), None)
-        # step counter (slots 0, 1) of the stochastic rounding of 16-bit storage,
-        # reset whenever the populations are set; slot 2: kernel status word
-        self._seed = torch.zeros(4, dtype=torch.int32, device=self.device)
+        # Small device words, read back in one copy by _check_health:
+        #   int32 view of int64 [0:2] -- slots 0, 1: step counter of the stochastic rounding of
+        #     16-bit storage (reset whenever the populations are set); slot 2: kernel status word;
+        #   int64 [2:4] -- health words (first bad node, non-finite flag);
+        #   int64 [4] -- the float64 bits of the last checked step's sum of f~* over fluid nodes.
+        self._words = torch.zeros(5, dtype=torch.int64, device=self.device)
+        self._seed = self._words[:2].view(torch.int32)
+        self._health = self._words[2:4]
         self.physics.round_seed = N.ptr(self._seed)
+        self.mass = None
+        """Total mass (sum of rho over fluid nodes, float64, summed on the device) of the state
+        after the last check of the run loop; None before the first."""
+        self._health_fresh = False
 
         # ---- immersed boundary and link rules -> special nodes
         self._ibm = None
@@ -294,7 +308,8 @@ class CudaSolver(Solver):
         # ---- populations
         self._f = torch.empty((q, self.qstride), dtype=self.t_store, device=self.device)
         self._f_next = torch.empty_like(self._f) if variant == "pull" else None
-        self._health = torch.empty(2, dtype=torch.int64, device=self.device)
+        self._n_fluid = int((~self._solid_host).sum())
+        self._setup_checked_launches()
         self.initialize()
 
     # ------------------------------------------------------------------ helpers
@@ -466,6 +481,21 @@ class CudaSolver(Solver):
         t["rule_row"] = torch.from_numpy(rule_row.astype(np.int32)).to(dev)
         t["rule_dense"] = torch.from_numpy(dense).to(dev, self.t_real)
 
+    def _setup_checked_launches(self) -> None:
+        """Launch descriptors of the checked step (health epilogue) and its partial-sum buffer."""
+        torch = self.torch
+        fused = self.launch_mode == "fused" and self._special.n_special > 0
+        probe = self._launches[N.LAUNCH_FUSED if fused else N.LAUNCH_BULK]
+        sp = self._special_struct()
+        n = N.load().lbm_health_partials(N.C.byref(self.grid), N.C.byref(sp), N.C.byref(probe))
+        if n <= 0:
+            raise N.NativeError(f"lbm_health_partials: invalid arguments (status {n})")
+        self._health_partial = torch.empty(int(n), dtype=torch.float64, device=self.device)
+        self._health_struct = N.Health(N.ptr(self._health), N.ptr(self._health_partial), int(n))
+        bx, by = self.block
+        self._checked_launches = {m: N.Launch(bx, by, m, 0, N.C.pointer(self._health_struct))
+                                  for m in N.LAUNCH_MODES}
+
     def _special_struct(self, export_in=None, export_out=None) -> N.Special:
         s = self._special
         t = s.tensors
@@ -575,7 +605,10 @@ class CudaSolver(Solver):
             self.time_step = int(z["time_step"])
 
     def _after_state_change(self):
-        self._seed[:2].zero_()
+        # step counter of the rounding, and the kernel status word: a fresh state
+        # starts with no report of an earlier step
+        self._seed[:3].zero_()
+        self._health_fresh = False
         s = self._special
         if self.variant == "aa" and s.n_export:
             self._export_cur = s.tensors["export_a"]
@@ -606,7 +639,7 @@ class CudaSolver(Solver):
         return self._f
 
     # ------------------------------------------------------------------ stepping
-    def _step_launch(self, name, sp, *tail, before_boundary=None):
+    def _step_launch(self, name, sp, *tail, before_boundary=None, checked=False):
         """One time step: a fused launch, or bulk + boundary kernels forked onto two streams.
 
         ``before_boundary(stream)`` (the immersed-boundary force of a pull step) runs first: on the side
@@ -614,11 +647,12 @@ class CudaSolver(Solver):
         kernel, which neither reads nor writes what it touches; else ahead of the step on this stream.
         """
         g, ph = N.C.byref(self.grid), N.C.byref(self.physics)
+        launches = self._checked_launches if checked else self._launches
         if self.launch_mode == "fused" or self._special.n_special == 0:
             if before_boundary is not None:
                 before_boundary(self._stream())
             mode = N.LAUNCH_FUSED if (self._special.n_special and self.launch_mode == "fused") else N.LAUNCH_BULK
-            self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[mode]), N.ptr(self._kind), *tail,
+            self._native(name, g, ph, N.C.byref(sp), N.C.byref(launches[mode]), N.ptr(self._kind), *tail,
                          self._stream())
             return
         torch = self.torch
@@ -629,10 +663,10 @@ class CudaSolver(Solver):
         side.wait_event(fork)
         if before_boundary is not None:
             before_boundary(side.cuda_stream)
-        self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[N.LAUNCH_BOUNDARY]), N.ptr(self._kind), *tail,
+        self._native(name, g, ph, N.C.byref(sp), N.C.byref(launches[N.LAUNCH_BOUNDARY]), N.ptr(self._kind), *tail,
                      side.cuda_stream)
         join.record(side)
-        self._native(name, g, ph, N.C.byref(sp), N.C.byref(self._launches[N.LAUNCH_BULK]), N.ptr(self._kind), *tail,
+        self._native(name, g, ph, N.C.byref(sp), N.C.byref(launches[N.LAUNCH_BULK]), N.ptr(self._kind), *tail,
                      main.cuda_stream)
         main.wait_event(join)
 
@@ -643,22 +677,23 @@ class CudaSolver(Solver):
             s = self._side = self.torch.cuda.Stream(self.device)
         return s
 
-    def _launch_pull(self):
+    def _launch_pull(self, checked=False):
         # the immersed-boundary force reads f_src only and feeds only the boundary kernel
         f = self._f
         ibm = None if self._ibm is None else (lambda stream: self._ibm.run(f, N.LAYOUT_PULL, stream))
         sp = self._special_struct()
-        self._step_launch("lbm_step_pull", sp, N.ptr(self._f), N.ptr(self._f_next), before_boundary=ibm)
+        self._step_launch("lbm_step_pull", sp, N.ptr(self._f), N.ptr(self._f_next), before_boundary=ibm,
+                          checked=checked)
         self._f, self._f_next = self._f_next, self._f
 
-    def _launch_aa(self, parity, layout):
+    def _launch_aa(self, parity, layout, checked=False):
         if self._ibm is not None:
             self._ibm.run(self._f, layout)
         ex_in = ex_out = None
         if self._special.n_export:
             ex_in, ex_out = self._export_cur, self._export_nxt
         sp = self._special_struct(ex_in, ex_out)
-        self._step_launch("lbm_step_aa", sp, N.ptr(self._f), parity)
+        self._step_launch("lbm_step_aa", sp, N.ptr(self._f), parity, checked=checked)
         if self._special.n_export:
             self._export_cur, self._export_nxt = self._export_nxt, self._export_cur
 
@@ -673,9 +708,29 @@ class CudaSolver(Solver):
 
     GRAPH_CHUNK = 32
 
+    def _advance_checked(self, steps: int) -> None:
+        """``_advance``, with the state check fused into the last step (the even half of the
+        last AA pair): its kernels also flag bad nodes and sum f~* in float64, and
+        ``_check_health`` reads the three words instead of scanning the lattice again."""
+        if steps <= 0:
+            return
+        m = self.step_multiple
+        self._advance(steps - m)
+        stream = self._stream()
+        self._native("lbm_health_reset", N.ptr(self._health), stream)
+        if self.variant == "aa":
+            self._launch_aa(N.LBM_AA_ODD, N.LAYOUT_AA_ODD)
+            self._launch_aa(N.LBM_AA_EVEN, N.LAYOUT_AA_EVEN, checked=True)
+        else:
+            self._launch_pull(checked=True)
+        mass_bits = self._words[4:5]  # float64 written through its int64 storage
+        self._native("lbm_health_finish", N.C.byref(self._health_struct), N.ptr(mass_bits), stream)
+        self._health_fresh = True
+
     def _advance(self, steps: int) -> None:
         if steps <= 0:
             return
+        self._health_fresh = False
         if not self.use_graph or steps < self.GRAPH_CHUNK:
             self._launch_steps(steps)
             return
@@ -715,11 +770,22 @@ class CudaSolver(Solver):
 
     # ------------------------------------------------------------------ readouts
     def _check_health(self) -> None:
-        """Device watchdog (reference ``solver.py:162-172``); raises ``SimulationDiverged``."""
-        self._native("lbm_health_reset", N.ptr(self._health), self._stream())
-        self._native("lbm_health", N.C.byref(self.grid), N.ptr(self._kind), N.ptr(self._f), N.ptr(self._health), self._stream())
-        first, nonfinite = (int(v) for v in self._health.cpu().tolist())
-        if int(self._seed[2].item()) != 0:
+        """Device watchdog (reference ``solver.py:162-172``); raises ``SimulationDiverged``.
+
+        After ``_advance_checked`` (the run loop) the last step has already checked the state
+        and summed its mass: one read of five words. Otherwise a separate scan of the lattice.
+        """
+        fused = self._health_fresh
+        if not fused:
+            self._native("lbm_health_reset", N.ptr(self._health), self._stream())
+            self._native("lbm_health", N.C.byref(self.grid), N.ptr(self._kind), N.ptr(self._f), N.ptr(self._health),
+                         self._stream())
+        words = self._words.cpu().numpy()
+        first, nonfinite = int(words[2]), int(words[3])
+        if fused:
+            self.mass = self._n_fluid + float(words[4:5].view(np.float64)[0])
+        if int(words[:2].view(np.int32)[2]) != 0:
+            self._seed[2].zero_()  # reported once; the state itself stays suspect until it is set again
             raise N.NativeError("a step kernel gave up waiting for its staged tiles (TMA loads did not arrive)")
         if first == 2**63 - 1:
             return

@@ -138,11 +138,38 @@ typedef struct lbm_special {
  * three give the same bits. lbm_step_aa chooses the same way, its TMA-staged
  * halves taking nx in [64, 256]. */
 enum { LBM_LAUNCH_FUSED = 0, LBM_LAUNCH_BULK = 1, LBM_LAUNCH_BOUNDARY = 2 };
+
+/* Health and mass check fused into a step (the step that ends a chunk of the
+ * run loop) -- replaces the separate scan of Solver._check_health
+ * (src/lbm/solver.py:162-172) over the state that step stores. Every fluid
+ * node the launch updates checks its stored post-collision populations:
+ * drho = sum_i f~*_i (direction order, the values as stored), bad if
+ * non-finite or drho <= -1; and the launch sums f~* over its nodes in
+ * float64, one partial sum per block, in a fixed order. */
+typedef struct lbm_health {
+    int64_t* words;      /* [0] smallest pitched index of a bad node (INT64_MAX: none), [1] 1 if a bad
+                            node is non-finite; set both with lbm_health_reset before the step */
+    double* partial;     /* n_partial doubles, written by the step (one per block) */
+    int64_t n_partial;   /* exactly lbm_health_partials(grid, sp, launch) for the step's launch mode */
+} lbm_health_t;
+
 typedef struct lbm_launch {
     int32_t tile_x;   /* multiple of 32 */
     int32_t tile_y;   /* tile_x * tile_y <= 256 */
     int32_t mode;     /* LBM_LAUNCH_* */
+    uint32_t tma_wait_limit; /* TMA-staged kernels: polls of the wait for a tile's staged loads before
+                                the block gives up (status word bit 0, see round_seed); 0 = the default,
+                                2^22 polls; LBM_TMA_WAIT_NONE = no poll at all, so every block gives up
+                                at its first tile (to exercise the time-out path). The block's final
+                                wait for loads still in flight always takes the default, so that none
+                                is left in flight when it exits. */
+    const lbm_health_t* health; /* NULL: a plain step. Else a checked step (lbm_step_pull, or lbm_step_aa
+                                   with parity LBM_AA_EVEN; LBM_ERR_INVALID for the odd half): the bulk
+                                   launch takes the one-node kernel whatever the storage (all bulk
+                                   kernels give the same bits); split launches (BULK + BOUNDARY) take
+                                   the same lbm_health_t and fill disjoint partial slots. */
 } lbm_launch_t;
+#define LBM_TMA_WAIT_NONE 0xFFFFFFFFu
 
 /* ---- the time step ---------------------------------------------------- */
 
@@ -205,6 +232,16 @@ int lbm_macroscopic(const lbm_grid_t* grid, const lbm_physics_t* phys, const uin
                     const void* f, int32_t layout, const int64_t* local_nodes, const void* local_force,
                     int32_t n_local, void* rho, void* u, lbm_stream_t stream);
 
+/* Partial slots a checked step with this launch writes (see lbm_health_t):
+ * FUSED: one per block of the fused grid; BULK or BOUNDARY: the bulk grid's
+ * blocks then the boundary launch's. Negative: invalid arguments. */
+int64_t lbm_health_partials(const lbm_grid_t* grid, const lbm_special_t* sp, const lbm_launch_t* launch);
+
+/* After a checked step (both launches, when split): delta_mass[0] = the sum of
+ * h->partial[0 .. n_partial) in a fixed order, float64 -- the sum of f~* over
+ * the fluid nodes, i.e. the mass minus the number of fluid nodes. */
+int lbm_health_finish(const lbm_health_t* h, double* delta_mass, lbm_stream_t stream);
+
 /* Divergence watchdog -- replaces Solver._check_health (src/lbm/solver.py:162-172).
  * out[0] = smallest pitched index of a fluid node with non-finite populations
  * or rho <= 0 (INT64_MAX if none); out[1] = 1 if any node is non-finite.
@@ -242,7 +279,9 @@ int lbm_affine_reduce(int32_t storage, const void* f, const int64_t* slots, cons
  * LBM_ERR_TOO_LARGE and launches nothing (use lbm_affine_reduce instead).
  * Set-up: the first call on each device, made with that device current,
  * looks up the array's address and caches it (this may load the library's
- * device code); make that first call before any stream capture.
+ * device code); make that first call before any stream capture. The cache
+ * belongs to the device's current context: after cudaDeviceReset the first
+ * call in the new context looks the address up again (same rule on capture).
  * Calls share one array per device: calls that may overlap in time on the
  * same device (different streams, or host threads without ordering) race
  * and give wrong sums; issue them on one stream. Each call clears the block

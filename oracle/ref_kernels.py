@@ -28,6 +28,7 @@ launch the link-rule pre-pass of that launch's layout (``rules_evaluate``,
 from __future__ import annotations
 
 import ctypes
+import os
 import shutil
 import subprocess
 import sys
@@ -35,7 +36,10 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REFERENCE_SRC = Path("/root/reference/src")
+DEFAULT_REFERENCE_SRC = "/root/reference/src"
+REFERENCE_SRC = Path(os.environ.get("LBM_REFERENCE_SRC", DEFAULT_REFERENCE_SRC))
+"""The reference's ``src`` directory (the ``LBM_REFERENCE_SRC`` environment variable, else the
+build container's read-only checkout)."""
 KERNELS = REFERENCE_SRC / "lbm" / "backends" / "kernels"
 LATTICES = ("D2Q9", "D3Q19")
 DTYPES = {"float32": "float", "float64": "double"}

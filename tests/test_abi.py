@@ -82,3 +82,20 @@ def test_solver_without_gpu_raises_backend_unavailable():
         pytest.skip("checks the error raised on machines without a GPU")
     with pytest.raises(lbm.BackendUnavailable):
         lbm.make_solver(lbm.SimulationParams(nx=8, ny=8, tau=0.8))
+
+
+def test_checked_step_partial_count_without_a_gpu():
+    """lbm_health_partials is host arithmetic: the bulk grid's blocks, then the boundary warps'
+    (split) or the fused grid's extra planes."""
+    lib = N.load()
+    grid = N.Grid(N.LBM_D3Q19, N.LBM_F32, 64, 20, 16, 64, 64 * 20 * 16)
+    sp = N.Special()
+    bulk = N.Launch(32, 4, N.LAUNCH_BULK)
+    assert lib.lbm_health_partials(ctypes.byref(grid), ctypes.byref(sp), ctypes.byref(bulk)) == 2 * 5 * 16
+    sp.n_special = 100
+    sp.node = sp.rule_mask = sp.rule_first = sp.force_slot = 8  # non-null; never dereferenced here
+    assert lib.lbm_health_partials(ctypes.byref(grid), ctypes.byref(sp), ctypes.byref(bulk)) == 160 + 4
+    fused = N.Launch(32, 4, N.LAUNCH_FUSED)
+    assert lib.lbm_health_partials(ctypes.byref(grid), ctypes.byref(sp), ctypes.byref(fused)) == 2 * 5 * 17
+    bad = N.Launch(48, 4, N.LAUNCH_BULK)
+    assert lib.lbm_health_partials(ctypes.byref(grid), ctypes.byref(sp), ctypes.byref(bad)) == N.LBM_ERR_INVALID

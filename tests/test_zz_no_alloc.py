@@ -87,3 +87,27 @@ def test_static_reduce_rejects_more_rows_than_its_scratch_holds():
         N.check(status, "lbm_affine_reduce_static")
     torch.cuda.synchronize()
     assert torch.count_nonzero(out).item() == 0  # nothing was launched
+
+
+@pytest.mark.parametrize("change", [
+    {"n_rows": 0}, {"n_rows": -5}, {"d": 0}, {"d": 4}, {"storage": 7}, {"storage": -1}, {"n_terms": -1},
+    {"null": 0}, {"null": 1}, {"null": 2}, {"null": 3}, {"null": 4}, {"out_null": True},
+])
+def test_static_reduce_rejects_invalid_arguments_and_launches_nothing(change):
+    """Every early return: LBM_ERR_INVALID and an untouched output (nothing is launched)."""
+    import torch
+
+    lib = N.load()
+    torch.cuda.set_device(0)
+    args = [N.ptr(t) for t in probe_inputs("float64", 4, 2, 3, seed=2)]
+    if "null" in change:
+        args[change["null"]] = None
+    n_rows, n_terms, d = change.get("n_rows", 4), change.get("n_terms", 2), change.get("d", 3)
+    storage = change.get("storage", N.LBM_F64)
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    status = lib.lbm_affine_reduce_static(storage, *args, n_rows, n_terms, d,
+                                          None if change.get("out_null") else N.ptr(out),
+                                          torch.cuda.current_stream().cuda_stream)
+    assert status == N.LBM_ERR_INVALID
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(out).item() == 0
