@@ -641,6 +641,23 @@ def run_ours(args, rank, world, local_rank):
     mlups = whole_job_mlups(nodes, steps, ms, world)
     ms_step = ms / steps
 
+    # ---- the public run loop: the state check (NaN / rho <= 0 scan, float64 mass) fused into the
+    # last step of every check_every-step chunk, read back with one small copy per chunk
+    run_loop = None
+    if world == 1:
+        loop_steps, check_every = 2000, 500
+        loop_steps += loop_steps % solver.step_multiple
+        solver.run(check_every, check_every=check_every)  # warm: the checked-step kernel
+        barrier()
+        start.record(stream)
+        solver.run(loop_steps, check_every=check_every)
+        stop.record(stream)
+        stop.synchronize()
+        loop_ms = start.elapsed_time(stop) / loop_steps
+        run_loop = {"ms_per_step": round(loop_ms, 5), "steps": loop_steps, "check_every": check_every,
+                    "vs_plain_steps": round(loop_ms / ms_step, 4), "mass": solver.mass,
+                    "what": "solver.run(steps, check_every) through the public API; CUDA events"}
+
     # ---- end to end through the public API, host buffers in pinned memory
     e2e = None
     if not args.no_e2e:
@@ -696,6 +713,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if run_loop is not None:
+        line["run_loop"] = run_loop
     if args.precision_steps > 0 and world == 1:
         del solver
         torch.cuda.empty_cache()

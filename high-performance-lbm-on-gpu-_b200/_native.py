@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -25,6 +25,8 @@ IBM_FUSED_MAX = 4096
 LBM_D2Q9, LBM_D3Q19 = 0, 1
 LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
 LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
+COLLIDE_TRT, COLLIDE_REGULARIZED = 0, 1
+COLLISION_CODE = {"bgk": COLLIDE_TRT, "trt": COLLIDE_TRT, "regularized": COLLIDE_REGULARIZED}
 LAYOUT_PULL, LAYOUT_AA_ODD, LAYOUT_AA_EVEN = 0, 1, 2
 KIND_SOLID, KIND_SPECIAL, KIND_NEAR, KIND_EDGE = 1, 2, 4, 8
 LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY = 0, 1, 2
@@ -53,7 +55,7 @@ class Grid(C.Structure):
 class Physics(C.Structure):
     _fields_ = [
         ("omega_plus", C.c_double), ("omega_minus", C.c_double), ("force", C.c_double * 3),
-        ("wall_u", vp), ("force_field", vp), ("solid_nbr", vp), ("round_seed", vp),
+        ("wall_u", vp), ("force_field", vp), ("solid_nbr", vp), ("collision", i32), ("round_seed", vp),
     ]
 
 

@@ -52,6 +52,8 @@ class BatchedSolver:
             raise BackendUnavailable(str(exc)) from exc
         if not params_list:
             raise ValueError("a batch needs at least one domain")
+        if any(getattr(p, "collision", "bgk") == "regularized" for p in params_list):
+            raise ValueError("the batched step runs TRT/BGK collision only; use CudaSolver for 'regularized'")
         self.torch = torch
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         self.params = list(params_list)
@@ -186,7 +188,7 @@ class BatchedSolver:
         if self.wall_offsets[i] >= 0:
             wall = self._wall[self.wall_offsets[i] :]
         return N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(wall), None, N.ptr(self._nbr[self.kind_offsets[i]:]),
-                         N.ptr(self._seed))
+                         N.COLLIDE_TRT, N.ptr(self._seed))
 
     # ------------------------------------------------------------------ state
     def initialize(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0, domain: int | None = None) -> None:

@@ -80,6 +80,8 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
     a.force_field = p->force_field;
     a.nbr = p->solid_nbr;
     if (!a.nbr) return LBM_ERR_INVALID;
+    if (p->collision != LBM_COLLIDE_TRT && p->collision != LBM_COLLIDE_REGULARIZED) return LBM_ERR_INVALID;
+    a.collision = p->collision;
     // 16-bit storage rounds stochastically and needs the step counter
     const bool half = g->storage == LBM_F16 || g->storage == LBM_BF16;
     if (half && !p->round_seed) return LBM_ERR_INVALID;
@@ -152,7 +154,7 @@ extern "C" int lbm_step_aa(const lbm_grid_t* g, const lbm_physics_t* p, const lb
 
 extern "C" int64_t lbm_health_partials(const lbm_grid_t* g, const lbm_special_t* sp, const lbm_launch_t* launch)
 {
-    if (!grid_valid(g) || !launch || !special_valid(sp, false)) return LBM_ERR_INVALID;
+    if (!grid_valid(g) || !launch || (sp && sp->n_special < 0)) return LBM_ERR_INVALID;
     const int tx = launch->tile_x, ty = launch->tile_y, mode = launch->mode;
     if (tx <= 0 || ty <= 0 || tx % 32 != 0 || tx * ty > 256) return LBM_ERR_INVALID;
     if (mode < LBM_LAUNCH_FUSED || mode > LBM_LAUNCH_BOUNDARY) return LBM_ERR_INVALID;
@@ -174,4 +176,4 @@ extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t wh
 
 extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
 
-extern "C" int32_t lbm_abi_version(void) { return 5; }
+extern "C" int32_t lbm_abi_version(void) { return 6; }

@@ -533,6 +533,7 @@ static bool make_adj(AdjArgs& A, const lbm_grid_t* g, const lbm_physics_t* p, co
 {
     if (!g || !p || !adj || !kind || g->qstride < (int64_t)g->pitch * g->ny * g->nz || g->pitch < g->nx) return false;
     if (g->lattice == LBM_D2Q9 && g->nz != 1) return false;
+    if (p->collision != LBM_COLLIDE_TRT) return false;  // the transposed collision is TRT/BGK's
     StepArgs& a = A.a;
     a.nx = g->nx;
     a.ny = g->ny;

@@ -503,6 +503,111 @@ __device__ __forceinline__ void collide_node(R (&f)[L::Q], const Relax<R>& c, bo
         collide<L, R, SCALE_LOG2>(f, c, Fx, Fy, Fz, NodeGuo<L, R, SCALE_LOG2>{c, Fx, Fy, Fz});
 }
 
+// ---------------------------------------------------------------- regularised collision
+// Projective regularisation (J. Latt and B. Chopard, Math. Comput. Simul. 72
+// (2006) 165-168; T. Krueger et al., The Lattice Boltzmann Method, Springer
+// 2017, sec. 10.6.5): the non-equilibrium part f^neq = f - feq is replaced by
+// its projection on the Hermite polynomials up to second order before it
+// relaxes, which filters the higher-order (ghost) moments that destabilise
+// BGK/TRT at low viscosity. With H_i = c_i c_i - I/3 and cs^2 = 1/3:
+//   P(f^neq)_i = w_i [3 c_i . m1 + 4.5 H_i : Pi],  m1 = sum c f^neq,  Pi = sum c c f^neq
+// Guo forcing: u = (j + F/2)/rho, so m1 = -F/2 exactly, and the odd part of
+// the update, (1 - w-) P_odd + (1 - w-/2) 3 w c.F = 1.5 w c.F, does not depend
+// on the odd rate. On shifted populations (f~ = f - w):
+//   Pi = sum c c f~ - rho u u - drho I/3        (second-order feq moments are exact on D2Q9/D3Q19)
+//   f*_i = feq~_i + 1.5 w_i c_i.F + (1 - w+) 4.5 w_i (c_i.Pi.c_i - tr Pi/3)
+//          + (1 - w+/2) w_i (9 (c_i.u)(c_i.F) - 3 u.F)
+// feq~_i = w_i [drho + rho (3 cu + 4.5 cu^2 - 1.5 u.u)]. Every operation rounds
+// explicitly, as in collide(). Used with the one-node kernels (SCALE_LOG2 = 0).
+template <class L, class R>
+__device__ __forceinline__ R reg_dot(int i, R ax, R ay, R az)
+{
+    R v = R(0);
+    bool first = true;
+    if (L::cx(i) != 0) { v = L::cx(i) > 0 ? ax : v_neg(ax); first = false; }
+    if (L::cy(i) != 0) { v = first ? (L::cy(i) > 0 ? ay : v_neg(ay)) : (L::cy(i) > 0 ? v_add(v, ay) : v_sub(v, ay)); first = false; }
+    if (L::D == 3 && L::cz(i) != 0) v = first ? (L::cz(i) > 0 ? az : v_neg(az)) : (L::cz(i) > 0 ? v_add(v, az) : v_sub(v, az));
+    return v;
+}
+
+template <class L, class R>
+__device__ __forceinline__ void collide_regularized(R (&f)[L::Q], const Relax<R>& c, R Fx, R Fy, R Fz)
+{
+    // moments of the streamed populations: drho, j, sum c c f~
+    R drho = f[0], jx = R(0), jy = R(0), jz = R(0);
+    R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        drho = v_add(drho, f[i]);
+        const int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
+        if (cx) { jx = cx > 0 ? v_add(jx, f[i]) : v_sub(jx, f[i]); sxx = v_add(sxx, f[i]); }
+        if (cy) { jy = cy > 0 ? v_add(jy, f[i]) : v_sub(jy, f[i]); syy = v_add(syy, f[i]); }
+        if (L::D == 3 && cz) { jz = cz > 0 ? v_add(jz, f[i]) : v_sub(jz, f[i]); szz = v_add(szz, f[i]); }
+        if (cx && cy) sxy = cx * cy > 0 ? v_add(sxy, f[i]) : v_sub(sxy, f[i]);
+        if (L::D == 3 && cx && cz) sxz = cx * cz > 0 ? v_add(sxz, f[i]) : v_sub(sxz, f[i]);
+        if (L::D == 3 && cy && cz) syz = cy * cz > 0 ? v_add(syz, f[i]) : v_sub(syz, f[i]);
+    }
+    const R half = R(0.5);
+    const R rho = v_add(R(1), drho);
+    const R inv = v_rcp(rho);
+    const R ux = v_mul(v_fma(half, Fx, jx), inv);
+    const R uy = v_mul(v_fma(half, Fy, jy), inv);
+    const R uz = L::D == 3 ? v_mul(v_fma(half, Fz, jz), inv) : R(0);
+    R usq = v_mul(ux, ux);
+    usq = v_fma(uy, uy, usq);
+    if (L::D == 3) usq = v_fma(uz, uz, usq);
+    R uF = v_mul(ux, Fx);
+    uF = v_fma(uy, Fy, uF);
+    if (L::D == 3) uF = v_fma(uz, Fz, uF);
+    // Pi = S - rho u u - drho/3 I
+    const R d3 = v_mul(drho, R(1.0 / 3.0));
+    const R pxx = v_sub(v_sub(sxx, v_mul(v_mul(rho, ux), ux)), d3);
+    const R pyy = v_sub(v_sub(syy, v_mul(v_mul(rho, uy), uy)), d3);
+    const R pzz = L::D == 3 ? v_sub(v_sub(szz, v_mul(v_mul(rho, uz), uz)), d3) : R(0);
+    const R pxy = v_sub(sxy, v_mul(v_mul(rho, ux), uy));
+    const R pxz = L::D == 3 ? v_sub(sxz, v_mul(v_mul(rho, ux), uz)) : R(0);
+    const R pyz = L::D == 3 ? v_sub(syz, v_mul(v_mul(rho, uy), uz)) : R(0);
+    R tr3 = v_add(pxx, pyy);
+    if (L::D == 3) tr3 = v_add(tr3, pzz);
+    tr3 = v_mul(tr3, R(1.0 / 3.0));
+    const R keep = c.one_m_wp;                        // 1 - w+
+    const R src = v_sub(R(1), v_mul(R(0.5), c.wp));   // 1 - w+/2
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        const int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
+        const R w = R(L::w(i));
+        const R cu = reg_dot<L, R>(i, ux, uy, uz);
+        const R cF = reg_dot<L, R>(i, Fx, Fy, Fz);
+        // c.Pi.c over the nonzero components of c (c_a^2 = 1)
+        R cpc = R(0);
+        if (cx) cpc = v_add(cpc, pxx);
+        if (cy) cpc = v_add(cpc, pyy);
+        if (L::D == 3 && cz) cpc = v_add(cpc, pzz);
+        if (cx && cy) cpc = cx * cy > 0 ? v_fma(R(2), pxy, cpc) : v_fma(R(-2), pxy, cpc);
+        if (L::D == 3 && cx && cz) cpc = cx * cz > 0 ? v_fma(R(2), pxz, cpc) : v_fma(R(-2), pxz, cpc);
+        if (L::D == 3 && cy && cz) cpc = cy * cz > 0 ? v_fma(R(2), pyz, cpc) : v_fma(R(-2), pyz, cpc);
+        const R qpi = v_sub(cpc, tr3);
+        // feq~ = w (drho + rho (3 cu + 4.5 cu^2 - 1.5 usq))
+        const R poly = v_fma(v_mul(R(4.5), cu), cu, v_fma(R(3), cu, v_mul(R(-1.5), usq)));
+        R out = v_mul(w, v_fma(rho, poly, drho));
+        out = v_fma(v_mul(R(1.5), w), cF, out);
+        out = v_fma(v_mul(v_mul(R(4.5), w), keep), qpi, out);
+        const R s_even = v_fma(v_mul(R(9), cu), cF, v_mul(R(-3), uF));
+        out = v_fma(v_mul(w, src), s_even, out);
+        f[i] = out;
+    }
+}
+
+// The node update of collision model CM (LBM_COLLIDE_*): TRT/BGK or regularised.
+template <class L, class R, int CM>
+__device__ __forceinline__ void collide_model(R (&f)[L::Q], const Relax<R>& c, bool uniform, R Fx, R Fy, R Fz)
+{
+    if constexpr (CM == LBM_COLLIDE_REGULARIZED)
+        collide_regularized<L, R>(f, c, Fx, Fy, Fz);
+    else
+        collide_node<L, R>(f, c, uniform, Fx, Fy, Fz);
+}
+
 // Moving-wall (Ladd) term 6 w_i (c_i . u_w) with u_w read at solid node s,
 // in explicitly rounded operations (added with v_add by every caller), so
 // every kernel that applies it gives the same bits.
@@ -537,6 +642,7 @@ struct StepArgs {
     uint32_t* seed;
     int parity;
     uint32_t wait_limit;  // polls of a TMA-staged block's wait for a tile (lbm_launch_t.tma_wait_limit)
+    int collision;        // LBM_COLLIDE_* (the kernels are instantiated per model)
     // Health and mass epilogue of a checked step (lbm_launch_t.health; null words: off).
     int64_t* health_words;    // [0] first bad pitched node (atomicMin), [1] 1 if non-finite (atomicMax)
     double* health_partial;   // one float64 sum per block of the launch

@@ -53,7 +53,7 @@ __device__ __forceinline__ void load4(const double* p, double (&c)[4])
     c[3] = q1.y;
 }
 
-template <class L, int ST, int VAR>
+template <class L, int ST, int VAR, int CM = LBM_COLLIDE_TRT>
 struct StepKernel {
     using S = Storage<ST>;
     using T = typename S::T;
@@ -207,7 +207,7 @@ struct StepKernel {
             Fy += ff[qs + nd];
             if (L::D == 3) Fz += ff[2 * qs + nd];
         }
-        collide_node<L, R>(f, a.template relax<R>(), a.guo_const && a.force_field == nullptr, Fx, Fy, Fz);
+        collide_model<L, R, CM>(f, a.template relax<R>(), a.guo_const && a.force_field == nullptr, Fx, Fy, Fz);
         const uint32_t h = S::STOCHASTIC ? sr_pair_hash(pair, a.seed[a.parity]) : 0u;
         if constexpr (H) stored_health(f, h, hi, nd, *hl);
         T* fd = static_cast<T*>(a.f_dst) + nd;
@@ -307,7 +307,7 @@ struct StepKernel {
                 if (L::D == 3) Fz += lf[2 * n + fs];
             }
         }
-        collide_node<L, R>(f, a.template relax<R>(), uniform, Fx, Fy, Fz);
+        collide_model<L, R, CM>(f, a.template relax<R>(), uniform, Fx, Fy, Fz);
         const uint32_t h = S::STOCHASTIC ? sr_pair_hash(sr_pair(a.nx, a.ny, x, y, z), a.seed[a.parity]) : 0u;
         const bool hi = x & 1;
         if constexpr (H) stored_health(f, h, hi, nd, *hl);
@@ -362,11 +362,11 @@ struct StepKernel {
 // path; in any other warp every lane takes the general path (interior lanes
 // with an empty mask), so no warp runs both paths one after the other.
 // Solid nodes are skipped, SPECIAL nodes are left to the boundary warps.
-template <class L, int ST, int VAR, bool H = false>
+template <class L, int ST, int VAR, bool H = false, int CM = LBM_COLLIDE_TRT>
 __device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z, int64_t nd, bool in,
                                           NodeHealth* hl = nullptr)
 {
-    using K = StepKernel<L, ST, VAR>;
+    using K = StepKernel<L, ST, VAR, CM>;
     const uint8_t k = in ? a.kind[nd] : KIND_SOLID;
     if (__all_sync(0xffffffffu, !in || k == KIND_FLUID)) {
         if (in) K::template interior<H>(a, nd, sr_pair(a.nx, a.ny, x, y, z), x & 1, hl);
@@ -377,12 +377,12 @@ __device__ __forceinline__ void bulk_node(const StepArgs& a, int x, int y, int z
 
 // Bulk: tile (blockIdx.x, blockIdx.y) of plane z; tile_x is a multiple of
 // 32, so every warp lies in one row.
-template <class L, int ST, int VAR, bool H = false>
+template <class L, int ST, int VAR, bool H = false, int CM = LBM_COLLIDE_TRT>
 __device__ __forceinline__ void bulk_tile(const StepArgs& a, int z, NodeHealth* hl = nullptr)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    bulk_node<L, ST, VAR, H>(a, x, y, z, ((int64_t)z * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny, hl);
+    bulk_node<L, ST, VAR, H, CM>(a, x, y, z, ((int64_t)z * a.ny + y) * a.pitch + x, x < a.nx && y < a.ny, hl);
 }
 
 // ---------------------------------------------------------------- vector pull
@@ -608,7 +608,7 @@ template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_B
 
 namespace lbm {
 
-template <class L, int ST, int VAR, bool H = false>
+template <class L, int ST, int VAR, bool H = false, int CM = LBM_COLLIDE_TRT>
 __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s, NodeHealth* hl = nullptr)
 {
     if (s >= a.sp.n_special) return;
@@ -617,7 +617,7 @@ __device__ __forceinline__ void boundary_node(const StepArgs& a, int64_t s, Node
     const int x = (int)(nd - row * a.pitch);
     const int y = (int)(row % a.ny);
     const int z = (int)(row / a.ny);
-    StepKernel<L, ST, VAR>::template node<true, H>(a, x, y, z, nd, a.nbr[nd], s, hl);
+    StepKernel<L, ST, VAR, CM>::template node<true, H>(a, x, y, z, nd, a.nbr[nd], s, hl);
 }
 
 // Bulk-only launches -- this kernel carries almost all of the traffic, so
@@ -638,38 +638,38 @@ constexpr int bulk_min_blocks()
     return 0;
 }
 
-template <class L, int ST, int VAR, bool H = false>
-__global__ void __launch_bounds__(256, bulk_min_blocks<ST, VAR, H>()) lbm_bulk_kernel(const StepArgs a)
+template <class L, int ST, int VAR, bool H = false, int CM = LBM_COLLIDE_TRT>
+__global__ void __launch_bounds__(256, bulk_min_blocks<ST, VAR, H || CM != LBM_COLLIDE_TRT>()) lbm_bulk_kernel(const StepArgs a)
 {
     advance_seed(a);
     if constexpr (H) {
         NodeHealth hl;
-        bulk_tile<L, ST, VAR, true>(a, blockIdx.z, &hl);
+        bulk_tile<L, ST, VAR, true, CM>(a, blockIdx.z, &hl);
         health_block(a, hl, ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
     } else {
-        bulk_tile<L, ST, VAR>(a, blockIdx.z);
+        bulk_tile<L, ST, VAR, false, CM>(a, blockIdx.z);
     }
 }
 
 // FUSED: grid (ceil(nx/bx), ceil(ny/by), nz + extra), planes z >= nz are
 // boundary warps. BOUNDARY: 1D grid over the list. Up to 255 registers, so
 // the general per-node path never spills.
-template <class L, int ST, int VAR, int MODE, bool H = false>
+template <class L, int ST, int VAR, int MODE, bool H = false, int CM = LBM_COLLIDE_TRT>
 __global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
 {
     NodeHealth hl;
     if (MODE == LBM_LAUNCH_BOUNDARY) {
-        boundary_node<L, ST, VAR, H>(a, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, &hl);
+        boundary_node<L, ST, VAR, H, CM>(a, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, &hl);
         if constexpr (H) health_block(a, hl, blockIdx.x);
         return;
     }
     const int z = blockIdx.z;
     if (z < a.nz) {
         advance_seed(a);
-        bulk_tile<L, ST, VAR, H>(a, z, &hl);
+        bulk_tile<L, ST, VAR, H, CM>(a, z, &hl);
     } else {
         const int64_t b = ((int64_t)(z - a.nz) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        boundary_node<L, ST, VAR, H>(a, b * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x, &hl);
+        boundary_node<L, ST, VAR, H, CM>(a, b * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x, &hl);
     }
     if constexpr (H) health_block(a, hl, ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
@@ -682,7 +682,7 @@ __global__ void __launch_bounds__(256, 1) lbm_step_kernel(const StepArgs a)
 // A checked step (health epilogue): the one-node bulk kernel, whatever the
 // storage (every bulk kernel gives the same bits), and boundary warps whose
 // per-block sums follow the bulk grid's in the partial array.
-template <class L, int ST, int VAR>
+template <class L, int ST, int VAR, int CM>
 static int launch_checked(StepArgs a, int mode, int tile_x, int tile_y, cudaStream_t stream)
 {
     if constexpr (VAR == LBM_AA_ODD) {
@@ -694,37 +694,39 @@ static int launch_checked(StepArgs a, int mode, int tile_x, int tile_y, cudaStre
             if (a.sp.n_special <= 0) return LBM_OK;
             a.health_slot0 = (int64_t)gx * gy * a.nz;
             const int64_t blocks = (a.sp.n_special + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS;
-            lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY, true><<<(unsigned)blocks, BOUNDARY_THREADS, 0, stream>>>(a);
+            lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY, true, CM><<<(unsigned)blocks, BOUNDARY_THREADS, 0, stream>>>(a);
         } else if (mode == LBM_LAUNCH_BULK) {
             if (a.nz > 65535) return LBM_ERR_INVALID;
             a.health_slot0 = 0;
-            lbm_bulk_kernel<L, ST, VAR, true><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+            lbm_bulk_kernel<L, ST, VAR, true, CM><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
         } else {
             const int64_t per_plane = (int64_t)gx * gy * tile_x * tile_y;
             const int64_t extra = a.sp.n_special > 0 ? (a.sp.n_special + per_plane - 1) / per_plane : 0;
             if (a.nz + extra > 65535) return LBM_ERR_INVALID;
             a.health_slot0 = 0;
-            lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED, true>
+            lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED, true, CM>
                 <<<dim3(gx, gy, (unsigned)(a.nz + extra)), dim3(tile_x, tile_y), 0, stream>>>(a);
         }
         return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
     }
 }
 
-template <class L, int ST, int VAR>
+// CM: the collision model; the node-pair and TMA-staged kernels implement
+// TRT/BGK only, so another model takes the one-node kernels.
+template <class L, int ST, int VAR, int CM = LBM_COLLIDE_TRT>
 static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cudaStream_t stream)
 {
-    if (a.health_words != nullptr) return launch_checked<L, ST, VAR>(a, mode, tile_x, tile_y, stream);
+    if (a.health_words != nullptr) return launch_checked<L, ST, VAR, CM>(a, mode, tile_x, tile_y, stream);
     const int threads = tile_x * tile_y;
     const unsigned gx = (unsigned)((a.nx + tile_x - 1) / tile_x);
     const unsigned gy = (unsigned)((a.ny + tile_y - 1) / tile_y);
     if (mode == LBM_LAUNCH_BOUNDARY) {
         if (a.sp.n_special <= 0) return LBM_OK;
         const int64_t blocks = (a.sp.n_special + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS;
-        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY><<<(unsigned)blocks, BOUNDARY_THREADS, 0, stream>>>(a);
+        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_BOUNDARY, false, CM><<<(unsigned)blocks, BOUNDARY_THREADS, 0, stream>>>(a);
     } else if (mode == LBM_LAUNCH_BULK) {
         if (a.nz > 65535) return LBM_ERR_INVALID;
-        if constexpr (VAR == LBM_PULL && has_vec<ST>()) {
+        if constexpr (VAR == LBM_PULL && has_vec<ST>() && CM == LBM_COLLIDE_TRT) {
             int status = LBM_OK;
             if (launch_tma<L, ST, LBM_PULL>(a, stream, &status)) return status;
             // pairs need every row and direction plane to start on an even
@@ -735,7 +737,7 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
                 return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
             }
         }
-        if constexpr (VAR != LBM_PULL && has_vec<ST>()) {
+        if constexpr (VAR != LBM_PULL && has_vec<ST>() && CM == LBM_COLLIDE_TRT) {
             int status = LBM_OK;
             if (launch_tma<L, ST, VAR>(a, stream, &status)) return status;
             // node pairs: every row and direction plane starts on an even node
@@ -745,12 +747,12 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
                 return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
             }
         }
-        lbm_bulk_kernel<L, ST, VAR><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+        lbm_bulk_kernel<L, ST, VAR, false, CM><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
     } else {
         const int64_t per_plane = (int64_t)gx * gy * threads;
         const int64_t extra = a.sp.n_special > 0 ? (a.sp.n_special + per_plane - 1) / per_plane : 0;
         if (a.nz + extra > 65535) return LBM_ERR_INVALID;
-        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED>
+        lbm_step_kernel<L, ST, VAR, LBM_LAUNCH_FUSED, false, CM>
             <<<dim3(gx, gy, (unsigned)(a.nz + extra)), dim3(tile_x, tile_y), 0, stream>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
@@ -760,6 +762,15 @@ template <class L, int ST>
 int launch_step(const StepArgs& a, int variant, int mode, int tile_x, int tile_y, cudaStream_t stream)
 {
     if (mode < LBM_LAUNCH_FUSED || mode > LBM_LAUNCH_BOUNDARY) return LBM_ERR_INVALID;
+    if (a.collision == LBM_COLLIDE_REGULARIZED) {
+        switch (variant) {
+        case LBM_PULL: return launch_mode<L, ST, LBM_PULL, LBM_COLLIDE_REGULARIZED>(a, mode, tile_x, tile_y, stream);
+        case LBM_AA_EVEN: return launch_mode<L, ST, LBM_AA_EVEN, LBM_COLLIDE_REGULARIZED>(a, mode, tile_x, tile_y, stream);
+        case LBM_AA_ODD: return launch_mode<L, ST, LBM_AA_ODD, LBM_COLLIDE_REGULARIZED>(a, mode, tile_x, tile_y, stream);
+        default: return LBM_ERR_INVALID;
+        }
+    }
+    if (a.collision != LBM_COLLIDE_TRT) return LBM_ERR_INVALID;
     switch (variant) {
     case LBM_PULL: return launch_mode<L, ST, LBM_PULL>(a, mode, tile_x, tile_y, stream);
     case LBM_AA_EVEN: return launch_mode<L, ST, LBM_AA_EVEN>(a, mode, tile_x, tile_y, stream);

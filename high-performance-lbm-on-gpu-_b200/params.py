@@ -19,7 +19,10 @@ import numpy as np
 from .lattice import LATTICES, VelocitySet, as_lattice, default_lattice
 
 TAU_WARNING = 0.51
-COLLISION_MODELS = ("bgk", "trt")
+COLLISION_MODELS = ("bgk", "trt", "regularized")
+"""The reference's two models and "regularized" (projective regularisation of the non-equilibrium
+part, Latt & Chopard 2006, with one relaxation rate 1/tau), which the reference lists on its
+roadmap (item 3, high Reynolds numbers) but does not implement."""
 SUPPORTED_DTYPES = ("float32", "float64", "float16", "bfloat16")
 COMPUTE_DTYPE = {"float32": "float32", "float64": "float64", "float16": "float32", "bfloat16": "float32"}
 """Arithmetic type of each storage format: 16-bit storage computes in float32."""
@@ -53,7 +56,7 @@ class SimulationParams:
     """Everything a solver needs to advance one simulation.
 
     Attributes follow the reference: ``nx, ny`` grid size; ``tau`` relaxation
-    time (> 1/2); ``collision`` ``"bgk"``/``"trt"``; ``magic`` the TRT
+    time (> 1/2); ``collision`` ``"bgk"``/``"trt"`` (or ``"regularized"``, an addition); ``magic`` the TRT
     parameter Lambda; ``force`` a uniform body-force density; ``solid`` the
     solid mask; ``wall_velocity`` (d, *shape), read only at solid nodes;
     ``dtype`` the population storage format; ``nz`` for 3D; ``lattice``;
@@ -150,6 +153,6 @@ class SimulationParams:
     def relaxation_rates(self) -> tuple[float, float]:
         """(omega_plus, omega_minus): 1/tau and 1/(1/2 + Lambda/(tau - 1/2)); equal for BGK."""
         omega_plus = 1.0 / self.tau
-        if self.collision == "bgk":
+        if self.collision in ("bgk", "regularized"):
             return omega_plus, omega_plus
         return omega_plus, 1.0 / (0.5 + self.magic / (self.tau - 0.5))

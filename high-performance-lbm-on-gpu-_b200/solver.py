@@ -281,7 +281,8 @@ class CudaSolver(Solver):
         self._force_field = None
         if force_field is not None:
             self._force_field = self._upload_field(np.asarray(force_field, dtype=np.float64).reshape(d, *shape))
-        self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field), None)
+        self.physics = N.Physics(wp, wm, (N.C.c_double * 3)(*force), N.ptr(self._wall), N.ptr(self._force_field), None,
+                                 N.COLLISION_CODE[params.collision])
         # Small device words, read back in one copy by _check_health:
         #   int32 view of int64 [0:2] -- slots 0, 1: step counter of the stochastic rounding of
         #     16-bit storage (reset whenever the populations are set); slot 2: kernel status word;
@@ -583,17 +584,29 @@ class CudaSolver(Solver):
         self._after_state_change()
 
     def save_checkpoint(self, path) -> None:
-        """Population-exact snapshot on disk (``.npz``): the populations in natural order, shape
-        (q, *shape), in the compute type (exact for every storage format), the time step and the step
-        counter of the stochastic rounding of 16-bit storage, so that a restored run continues bit
-        for bit (``load_checkpoint``)."""
+        """Population-exact snapshot on disk.
+
+        ``.npy``: the populations alone, natural direction order, shape (q, *shape), in the compute
+        type (exact for every storage format) -- the array ``populations()`` returns, which the
+        reference's solvers and the NumPy oracle hold as their state (reference ``solver.py:190-192``).
+        Any other suffix (``.npz``): the same populations plus the time step and the step counter of
+        the stochastic rounding of 16-bit storage, so that a restored run continues bit for bit.
+        """
+        if str(path).endswith(".npy"):
+            np.save(path, self.populations())
+            return
         counter = int(self._seed[:2].cpu().numpy().view(np.uint32).max())
         np.savez(path, populations=self.populations(), time_step=np.int64(self.time_step),
                  round_step=np.uint32(counter), dtype=np.str_(self.params.dtype), shape=np.asarray(self.shape),
                  lattice=np.str_(self.lattice.name))
 
     def load_checkpoint(self, path) -> None:
-        """Restore a ``save_checkpoint`` snapshot of a run with the same lattice, shape and storage."""
+        """Restore a ``save_checkpoint`` snapshot of a run with the same lattice, shape and storage
+        (a ``.npy`` of natural-order populations from any solver: the time step is left as it is
+        and the 16-bit rounding counter restarts at 0)."""
+        if str(path).endswith(".npy"):
+            self.set_populations(np.load(path))
+            return
         with np.load(path) as z:
             if (tuple(int(v) for v in z["shape"]) != tuple(self.shape) or str(z["dtype"]) != self.params.dtype
                     or str(z["lattice"]) != self.lattice.name):
@@ -816,6 +829,19 @@ class CudaSolver(Solver):
         return k * self.qstride + self._pitched(node)
 
     def _affine_tensors(self, compiled):
+        """Device slots, coefficients and constants of compiled expressions, uploaded once per
+        ``CompiledAffine`` object (a probe read every few steps keeps its tables on the device)."""
+        cache = self.__dict__.setdefault("_affine_cache", {})
+        hit = cache.get(id(compiled))
+        if hit is not None and hit[0] is compiled:
+            return hit[1]
+        if len(cache) >= 64:
+            cache.clear()
+        tensors = self._upload_affine(compiled)
+        cache[id(compiled)] = (compiled, tensors)
+        return tensors
+
+    def _upload_affine(self, compiled):
         torch = self.torch
         coeff = np.asarray(compiled.coeff, dtype=np.float64)
         if coeff.ndim == 1:
@@ -842,11 +868,18 @@ class CudaSolver(Solver):
         d = weight.shape[1]
         if rows == 0:
             return np.zeros(d)
-        w = torch.from_numpy(np.ascontiguousarray(weight)).to(self.device)
-        blocks = (rows + 255) // 256
-        partial = torch.empty(blocks * d, dtype=torch.float64, device=self.device)
-        counter = torch.zeros(1, dtype=torch.int32, device=self.device)
-        out = torch.empty(d, dtype=torch.float64, device=self.device)
+        key = ("reduce", id(compiled))
+        cache = self.__dict__.setdefault("_affine_cache", {})
+        hit = cache.get(key)
+        if hit is not None and hit[0] is compiled and np.array_equal(hit[2], weight):
+            w, partial, counter, out = hit[1]
+        else:
+            blocks = (rows + 255) // 256
+            w = torch.from_numpy(np.ascontiguousarray(weight)).to(self.device)
+            partial = torch.empty(blocks * d, dtype=torch.float64, device=self.device)
+            counter = torch.zeros(1, dtype=torch.int32, device=self.device)  # re-armed by every reduction
+            out = torch.empty(d, dtype=torch.float64, device=self.device)
+            cache[key] = (compiled, (w, partial, counter, out), np.array(weight))
         self._native("lbm_affine_reduce", self.grid.storage, N.ptr(self._f), N.ptr(slots), N.ptr(coeff), N.ptr(const),
                      N.ptr(w), rows, terms, d, N.ptr(partial), N.ptr(counter), N.ptr(out), self._stream())
         return out.cpu().numpy()

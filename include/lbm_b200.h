@@ -37,6 +37,13 @@ enum {
 enum { LBM_D2Q9 = 0, LBM_D3Q19 = 1 };
 enum { LBM_F32 = 0, LBM_F64 = 1, LBM_F16 = 2, LBM_BF16 = 3 };
 enum { LBM_PULL = 0, LBM_AA_EVEN = 1, LBM_AA_ODD = 2 };
+/* Collision model (lbm_physics_t.collision). TRT covers BGK (omega_minus == omega_plus).
+ * REGULARIZED: projective regularisation of the non-equilibrium part onto the
+ * second-order Hermite moments (Latt & Chopard 2006) before a single-rate
+ * relaxation with omega_plus, Guo forcing -- not in the reference (its roadmap
+ * item 3, README "High Reynolds numbers"); the one-node kernels run it
+ * whatever the storage, the adjoint and batched steps take TRT only. */
+enum { LBM_COLLIDE_TRT = 0, LBM_COLLIDE_REGULARIZED = 1 };
 /* Where a stored state keeps f*_k(y) (reference src/lbm/link_rules.py:16-25). */
 enum { LBM_LAYOUT_PULL = 0, LBM_LAYOUT_AA_ODD = 1, LBM_LAYOUT_AA_EVEN = 2 };
 /* Node kind bits (one byte per node): SOLID; SPECIAL (updated by the boundary
@@ -63,6 +70,7 @@ typedef struct lbm_physics {
     const void* force_field; /* real[d][qstride] per-node body force added to force[], or NULL */
     const uint32_t* solid_nbr; /* per node: bit i set where x - c_i is solid (lbm_classify); read only
                                   at fluid nodes that are not interior */
+    int32_t collision;     /* LBM_COLLIDE_* */
     uint32_t* round_seed;  /* float16/bfloat16 storage (required there, ignored otherwise): three
                               uint32 slots in device memory. Slots 0 and 1 hold the step counter of
                               the stochastic rounding of stored populations: a step reads slot p and

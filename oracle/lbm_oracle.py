@@ -164,6 +164,46 @@ def collide(lattice, f, wp, wm, force):
     return post
 
 
+def collide_regularized(lattice, f, wp, force):
+    """Regularised collision with Guo forcing on every node of f (q, ...).
+
+    Not in the reference (its roadmap item 3, README "High Reynolds numbers");
+    restated from the published method: projective regularisation, J. Latt and
+    B. Chopard, Math. Comput. Simul. 72 (2006) 165-168 (also T. Krueger et al.,
+    The Lattice Boltzmann Method, Springer 2017, sec. 10.6.5). The
+    non-equilibrium part f^neq = f - feq (feq as in ``equilibrium``, u = (j +
+    F/2)/rho) is replaced by its projection on the Hermite polynomials up to
+    second order, w_i [3 c_i . m1 + 4.5 (c_i c_i - I/3) : Pi] with m1 = sum c
+    f^neq and Pi = sum c c f^neq, which then relaxes at rate wp; the Guo source
+    is split as in ``guo_source``. Since m1 = -F/2, the odd part of the update
+    is 1.5 w c.F whatever the odd rate:
+        f*_i = feq_i + 1.5 w_i c_i.F + (1 - wp) 4.5 w_i (c_i.Pi.c_i - tr Pi / 3)
+               + (1 - wp/2) w_i (9 (c_i.u)(c_i.F) - 3 u.F)
+    """
+    d = lattice.d
+    drho = f.sum(axis=0)
+    rho = 1.0 + drho
+    u = tuple((ja + 0.5 * fa) / rho for ja, fa in zip(_momentum(lattice, f), force, strict=True))
+    neq = f - equilibrium(lattice, drho, u)
+    c = np.asarray(lattice.c)
+    pi = {}
+    for a in range(d):
+        for b in range(a, d):
+            pi[a, b] = sum(c[i, a] * c[i, b] * neq[i] for i in range(lattice.q) if c[i, a] * c[i, b])
+    trace = sum(pi[a, a] for a in range(d))
+    u_dot_f = sum(ua * fa for ua, fa in zip(u, force, strict=True))
+    out = []
+    for i, wi in enumerate(lattice.w):
+        ci = c[i]
+        cpc = sum(ci[a] * ci[b] * pi[min(a, b), max(a, b)] for a in range(d) for b in range(d) if ci[a] * ci[b])
+        cf = _dot(ci, force)
+        cu = _dot(ci, u)
+        feq = wi * (drho + rho * (3.0 * cu + 4.5 * cu * cu - 1.5 * sum(ua * ua for ua in u)))
+        out.append(feq + 1.5 * wi * cf + (1.0 - wp) * 4.5 * wi * (cpc - trace / 3.0)
+                   + (1.0 - 0.5 * wp) * wi * (9.0 * cu * cf - 3.0 * u_dot_f))
+    return np.stack(out).astype(f.dtype)
+
+
 def stream_pull(lattice, f):
     """f_i(x) = f*_i(x - c_i), periodic (``streaming.py:32-37``)."""
     axes = tuple(range(lattice.d))
@@ -352,7 +392,10 @@ class OracleSolver:
             target, slots, coeff, const = self.rules
             values = const + (coeff * f.reshape(-1)[slots]).sum(axis=1)
             streamed.reshape(-1)[target] = values
-        post = collide(lattice, streamed, self.rates[0], self.rates[1], force)
+        if getattr(self.params, "collision", "bgk") == "regularized":
+            post = collide_regularized(lattice, streamed, self.rates[0], force)
+        else:
+            post = collide(lattice, streamed, self.rates[0], self.rates[1], force)
         self.f = stochastic_round(np.where(self.fluid, post, f), self.dtype, self.round_step)
         self.round_step += 1
 

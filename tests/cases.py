@@ -146,6 +146,51 @@ def cylinder_channel(ns, method="bouzidi", nx=880, ny=164, dtype="float32", u_ma
     return params, links, inflow
 
 
+def schaefer_turek(ns, test="2D-2", n=20, u_max=0.05, dtype="float32", collision="trt"):
+    """The Schaefer-Turek DFG cylinder benchmark at N nodes per diameter, Bouzidi cylinder
+    (the reference's ``cases/cylinder_benchmark.py:93-130``, ``build``).
+
+    Channel H = 0.41, L = 2.2, D = 0.1 centred at (0.2, 0.2), nu = 1e-3 (SI); dx = D / N; the
+    x = 0 layer is the Zou-He velocity inlet acting at x = 1, the last layer the pressure outlet;
+    channel walls halfway at y = 0.5 and ny - 1.5. 2D-2: U_m = 1.5 m/s, Re = 100.
+    Returns (params, cylinder links, u_mean, inflow profile u_x(y)).
+    """
+    height_si, length_si, diameter_si, centre_si, nu_si = 0.41, 2.2, 0.1, (0.2, 0.2), 1e-3
+    u_m_si = {"2D-1": 0.3, "2D-2": 1.5}[test]
+    dx = diameter_si / n
+    ny = round(height_si / dx) + 2
+    nx = round(length_si / dx) + 3
+    height = ny - 2
+    y = np.arange(ny) - 0.5
+    profile = np.where((y > 0) & (y < height), 4.0 * u_max * y * (height - y) / height**2, 0.0)
+    inflow = np.stack([profile, np.zeros(ny)])
+    solid = np.zeros((ny, nx), dtype=bool)
+    solid[0, :] = solid[-1, :] = True
+    body = ns.circle(1.0 + centre_si[0] / dx, 0.5 + centre_si[1] / dx, 0.5 * n)
+    solid |= ns.voxelize(body, solid.shape)
+    lattice = ns.default_lattice(2)
+    solid, open_rules = ns.open_channel(lattice, solid, inflow)
+    links = ns.wall_links(lattice, body, solid)
+    rules = ns.LinkRules.concat(open_rules, ns.bouzidi_rules(lattice, links, solid))
+    u_mean = 2.0 * u_max / 3.0
+    reynolds = u_m_si * 2.0 / 3.0 * diameter_si / nu_si
+    nu = u_mean * n / reynolds
+    params = ns.SimulationParams(nx=nx, ny=ny, tau=3.0 * nu + 0.5, collision=collision, solid=solid, dtype=dtype,
+                                 link_rules=rules)
+    return params, links, u_mean, profile
+
+
+def lift_period(t, cl):
+    """Mean period of C_L(t) from its upward zero crossings, each located by linear interpolation
+    between the samples around it (the reference's ``cylinder_benchmark.lift_period``)."""
+    t, cl = np.asarray(t, dtype=np.float64), np.asarray(cl, dtype=np.float64)
+    up = np.flatnonzero((cl[:-1] < 0) & (cl[1:] >= 0))
+    if len(up) < 2:
+        raise ValueError("need at least two upward zero crossings of C_L to measure a period")
+    crossings = t[up] - cl[up] * (t[up + 1] - t[up]) / (cl[up + 1] - cl[up])
+    return float(np.mean(np.diff(crossings)))
+
+
 def sphere_channel(ns, nx=128, ny=64, nz=64, radius=8.0, u_in=0.04, tau=0.6, dtype="float32"):
     """Config: D3Q19 channel 128 x 64 x 64, Bouzidi sphere r = 8, Zou-He inlet U, outlet rho = 1."""
     lattice = ns.default_lattice(3)

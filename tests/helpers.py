@@ -20,6 +20,25 @@ NS = types.SimpleNamespace(
 """This package's builders, in the shape ``tests/cases.py`` expects."""
 
 
+def reference_ns():
+    """The reference's own builders (the unmodified package in baseline/_ref), in the shape
+    ``tests/cases.py`` expects; None where it is not installed."""
+    from oracle import reference_package
+
+    ref = reference_package.modules()
+    if ref is None:
+        return None
+    from lbm.boundaries import cavity_walls, channel_walls  # noqa: PLC0415
+
+    g, lk = ref.geometry, ref.link_rules
+    return types.SimpleNamespace(
+        SimulationParams=ref.params.SimulationParams, channel_walls=channel_walls, cavity_walls=cavity_walls,
+        circle=g.circle, sphere=g.sphere, voxelize=g.voxelize, wall_links=g.wall_links,
+        ImmersedBoundary=ref.ibm.ImmersedBoundary, default_lattice=ref.lattice.default_lattice,
+        LinkRules=lk.LinkRules, bouzidi_rules=lk.bouzidi_rules, open_channel=ref.open_boundaries.open_channel,
+    )
+
+
 def golden(name: str) -> dict:
     with np.load(GOLDEN / f"{name}.npz") as data:
         return {k: data[k] for k in data.files}

@@ -152,6 +152,67 @@ def test_cylinder_channel_matches_oracle(method):
         np.testing.assert_allclose(gpu.immersed_force, ref.immersed_force, rtol=1e-5, atol=1e-9)
 
 
+def run_schaefer_turek_2d2(backend, n=20, convective_times=150.0, samples_per_time=40):
+    """The reference's 2D-2 protocol (``cases/cylinder_benchmark.py:231-255``, ``run_periodic``):
+    start from the inflow profile, sample C_D and C_L ``samples_per_time`` times per convective
+    time D/U_mean through the run loop's callback, measure the last quarter of the record."""
+    p, links, u_mean, profile = cases.schaefer_turek(NS, "2D-2", n, dtype="float32")
+    s = lbm.make_solver(p, backend=backend)
+    s.initialize(1.0, np.where(p.solid, 0.0, profile[:, None]), 0.0)
+    probe = lbm.ForceProbe.build(p, links)
+    scale = 0.5 * u_mean**2 * n
+    t_conv = n / u_mean
+    every = max(2, 2 * round(t_conv / samples_per_time / 2))
+    total = every * round(convective_times * t_conv / every)
+    history = []
+    s.run(total, every=every, callback=lambda sv: history.append((sv.time_step, *(probe.evaluate(sv) / scale))))
+    h = np.asarray(history)
+    tail = h[len(h) * 3 // 4:]
+    strouhal = n / (cases.lift_period(tail[:, 0], tail[:, 2]) * u_mean)
+    return float(tail[:, 1].max()), float(tail[:, 2].max()), strouhal, h
+
+
+@pytest.mark.parametrize("backend", ["cuda-aa", "cuda-naive"])
+def test_schaefer_turek_2d2_shedding_frequency_lift_and_drag(backend):
+    """Periodic shedding behind the Bouzidi cylinder at Re = 100, N = 20, float32: the benchmark's
+    published intervals, with the reference's own validation tolerances
+    (``tests/validation/test_cylinder_benchmark.py:22-32``): 0.295 < St < 0.305,
+    C_L,max = 1.0 within 8 %, C_D,max = 3.23 within 3 %."""
+    cd_max, cl_max, strouhal, _ = run_schaefer_turek_2d2(backend)
+    assert 0.295 < strouhal < 0.305, strouhal
+    assert cl_max == pytest.approx(1.0, rel=0.08)
+    assert cd_max == pytest.approx(3.23, rel=0.03)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("method", ["bouzidi", "ibm"])
+def test_cylinder_config_force_series_matches_oracle(method):
+    """The cylinder configuration (880 x 164, D = 40, Re = 100, float32) from rest: C_D and C_L
+    sampled every 100 steps for 1000 steps -- the probe's momentum exchange (Bouzidi) or the
+    immersed body's force (IBM), float64 readouts -- against the oracle's, within 2e-3 of the
+    series' largest coefficient (float32 populations agree to ~1e-7; a force sums a few hundred
+    link terms)."""
+    p, links, _ = cases.cylinder_channel(NS, method, dtype="float32")
+    u_mean = 2.0 * 0.05 / 3.0
+    scale = 0.5 * u_mean**2 * 40.0
+    gpu = lbm.make_solver(p, backend="cuda-naive")
+    ref = OracleSolver(p)
+    probe = lbm.ForceProbe.build(p, links) if links is not None else None
+    got, want = [], []
+    for _ in range(10):
+        gpu.run(100)
+        ref.run(100)
+        if probe is not None:
+            got.append(probe.evaluate(gpu) / scale)
+            want.append(probe.weight.T @ ref.evaluate_affine(probe.compiled("reference")) / scale)
+        else:
+            got.append(gpu.immersed_force / scale)
+            want.append(ref.immersed_force / scale)
+    got, want = np.asarray(got), np.asarray(want)
+    assert np.abs(want).max() > 0.1  # the body feels the flow
+    np.testing.assert_allclose(got, want, rtol=0, atol=2e-3 * np.abs(want).max())
+
+
 # ---------------------------------------------------------------- batched cavities
 def test_batched_cavity_config_domains_match_single_runs():
     from lbm_b200.batched import BatchedSolver, cavity_batch
