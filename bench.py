@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched-cavities study (aggregate MLUPS against separate launches)")
-    ap.add_argument("--study", choices=("tgv", "cylinder", "batched", "adjoint", "precision"), default=None,
+    ap.add_argument("--study", choices=("tgv", "cylinder", "batched", "adjoint", "precision", "setup"), default=None,
                     help="run one configuration study alone and print its JSON (no duct line)")
     ap.add_argument("--study-steps", type=int, default=None, help="steps of --study (default: the study's own)")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
@@ -561,6 +561,45 @@ def batched_study(lbm, torch, steps: int = 640, separate_steps: int = 20):
             "steps": {"batched": steps, "separate": separate_steps}}
 
 
+def setup_study(lbm, torch):
+    """Set-up time of two bodies in a channel, host builders against the device-side compiler
+    (voxelisation, wall links, Bouzidi rules; the solver's own tables after): the sphere channel
+    (128 x 64 x 64, r = 8) and a 256^3 duct with a sphere of radius 40. Wall-clock seconds."""
+    from lbm_b200 import device_rules
+
+    out = {}
+    for label, shape, body in (("sphere_channel_128x64x64", (64, 64, 128), lbm.sphere(32.0, 31.5, 31.5, 8.0)),
+                               ("duct_256_sphere_r40", (256, 256, 256), lbm.sphere(256 / 3, 127.5, 127.5, 40.0))):
+        nz, ny, nx = shape
+        solid = lbm.duct_walls(nx, ny, nz)
+        lattice = lbm.D3Q19
+        device_rules.ball_channel(lattice, body, solid)  # warm: module load, first launches
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ds, dl, dr = device_rules.ball_channel(lattice, body, solid)
+        t_dev = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hs = solid | lbm.voxelize(body, solid.shape)
+        hl = lbm.wall_links(lattice, body, hs)
+        hr = lbm.bouzidi_rules(lattice, hl, hs)
+        t_host = time.perf_counter() - t0
+        same = bool(np.array_equal(ds, hs) and np.array_equal(dl.q, hl.q) and np.array_equal(dr.values.coeff, hr.values.coeff))
+        t0 = time.perf_counter()
+        params = lbm.SimulationParams(nx=nx, ny=ny, nz=nz, tau=0.6, collision="trt", solid=ds, link_rules=dr)
+        t_params = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        solver = lbm.make_solver(params, backend="cuda-naive")
+        torch.cuda.synchronize()
+        t_solver = time.perf_counter() - t0
+        out[label] = {"links": len(dl), "rules": len(dr), "host_builders_s": round(t_host, 3),
+                      "device_builders_s": round(t_dev, 4), "speedup": round(t_host / t_dev, 1),
+                      "identical": same, "params_validation_s": round(t_params, 3),
+                      "solver_tables_s": round(t_solver, 3)}
+        del solver
+        torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(x: float, world: int, device) -> float:
     """The largest value over all ranks (the slowest replica's time); x itself on one rank."""
     if world <= 1:
@@ -759,6 +798,8 @@ def run_study(args):
     elif args.study == "adjoint":
         kw = {"steps": k, "window": max(1, k // 4), "fd": False} if k else {}
         result = adjoint_study(lbm, torch, **kw)
+    elif args.study == "setup":
+        result = setup_study(lbm, torch)
     else:
         result = precision_study(lbm, torch, args.n, k or args.precision_steps, args.variant)
     print(json.dumps({"study": args.study, "result": result}), flush=True)

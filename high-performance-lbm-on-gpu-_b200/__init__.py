@@ -22,7 +22,7 @@ from __future__ import annotations
 
 import sys as _sys
 
-from . import build, diagnostics, forces, geometry, ibm, lattice, link_rules, open_boundaries, params
+from . import build, device_rules, diagnostics, forces, geometry, ibm, lattice, link_rules, open_boundaries, params
 from .diagnostics import MacroscopicFields
 from .forces import ForceProbe
 from .geometry import Ball, WallLinks, cavity_walls, channel_walls, circle, duct_walls, sphere, voxelize, wall_links

@@ -135,8 +135,13 @@ _SIGNATURES = {
     "lbm_ibm_adjoint_iteration": [P(Grid), P(Ibm), vp, vp, i32, C.c_double, vp, vp, vp],
     "lbm_ibm_adjoint_moments": [P(Grid), P(Ibm), vp, vp, vp],
     "lbm_kernel_resources": [i32, i32, i32, vp],
+    "lbm_ball_voxelize": [P(Grid), C.c_double, C.c_double, C.c_double, C.c_double, vp, vp],
+    "lbm_ball_links_count": [P(Grid), vp, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp],
+    "lbm_ball_links_write": [P(Grid), vp, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp, vp, vp, vp],
+    "lbm_bouzidi_links": [P(Grid), vp, i64, vp, vp, vp, vp, vp, vp, vp, vp],
+    "lbm_compile_terms": [P(Grid), i32, vp, vp, i64, vp, vp, vp, vp, vp, vp],
 }
-EXPORTED = (*_SIGNATURES, "lbm_health_partials", "lbm_last_cuda_error", "lbm_abi_version")
+EXPORTED = (*_SIGNATURES, "lbm_health_partials", "lbm_ball_links_scratch", "lbm_last_cuda_error", "lbm_abi_version")
 
 _lib = None
 
@@ -159,6 +164,8 @@ def load(path: Path | None = None):
         fn.restype = C.c_int
     lib.lbm_health_partials.argtypes = [P(Grid), P(Special), P(Launch)]
     lib.lbm_health_partials.restype = i64
+    lib.lbm_ball_links_scratch.argtypes = [P(Grid)]
+    lib.lbm_ball_links_scratch.restype = i64
     lib.lbm_last_cuda_error.restype = C.c_char_p
     lib.lbm_last_cuda_error.argtypes = []
     lib.lbm_abi_version.restype = i32

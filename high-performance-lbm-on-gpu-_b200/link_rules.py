@@ -20,8 +20,8 @@ layout         slot of f*_k(y)                             used for
 =============  ==========================================  ==================
 
 Slot index = k * n_nodes + node (unpadded). The CUDA solver applies rules
-inside its boundary warps (``csrc/step_*.cu``) instead of a pre-pass; see
-``solver.RuleTables`` for the device form.
+inside its boundary warps (``csrc/step_kernels.cuh``) instead of a pre-pass;
+``CudaSolver._build_special`` turns them into its per-node device tables.
 """
 
 from __future__ import annotations
@@ -198,50 +198,64 @@ class CompiledRules:
     values: CompiledAffine
 
 
-def compile_affine(lattice, values: AffineSet, layout: str, solid, wall_velocity) -> CompiledAffine:
-    """Flat slots of every term in ``layout`` (reference ``link_rules.py:203-240``).
+def _term_destinations(lattice, k, y, shape):
+    """Flat index of y + c_k (periodic) for every term at once; k, y of any common shape."""
+    c = np.asarray(lattice.c, dtype=np.int64)[k]  # (..., d), components x, y[, z]
+    coords = np.unravel_index(y, shape)           # (z,) y, x
+    d = len(shape)
+    moved = tuple((coords[a] + c[..., d - 1 - a]) % shape[a] for a in range(d))
+    return np.ravel_multi_index(moved, shape)
 
-    For ``aa_even`` a blocked push (y + c_k solid) left f*_k(y) reflected into
-    slot (opp k, y) with the moving-wall term of direction opp(k) added, so
-    the constant gains + 6 w_k (c_k . u_w) to undo it.
+
+def compile_affine(lattice, values: AffineSet, layout: str, solid, wall_velocity) -> CompiledAffine:
+    """Resolve every term f*_k(y) of ``values`` to a flat slot of the stored state in ``layout``.
+
+    Same slot semantics as the reference's compiler (``link_rules.py:203-240``; see the layout
+    table above), computed for all terms in one pass: ``reference``/``pull`` (k, y); ``aa_odd``
+    (opp k, y); ``aa_even`` (k, y + c_k), or, where y + c_k is solid, (opp k, y) -- the odd step
+    reflected f*_k(y) there with the moving-wall term 6 w_opp(k) (c_opp(k) . u_w) added, so each
+    such term contributes coeff 6 w_k (c_k . u_w(y + c_k)) to its row's constant (summed over the
+    row's terms in order). ``CudaSolver`` resolves the same slots on the device for its own
+    buffers (``lbm_compile_terms``).
     """
     if layout not in LAYOUTS:
         raise ValueError(f"unknown layout {layout!r}; choose from {LAYOUTS}")
-    shape = np.asarray(solid).shape
-    n_nodes = int(np.prod(shape))
+    solid = np.asarray(solid, dtype=bool)
+    shape = solid.shape
+    n = solid.size
     k = np.asarray(values.direction, dtype=np.int64)
     y = np.asarray(values.node, dtype=np.int64)
+    coeff = np.asarray(values.coeff, dtype=np.float64)
     constant = np.array(values.constant, dtype=np.float64, copy=True)
-    opposite = np.asarray(lattice.opposite)
+    opp = np.asarray(lattice.opposite, dtype=np.int64)
     if layout in ("reference", "pull"):
-        slots = k * n_nodes + y
-    elif layout == "aa_odd":
-        slots = opposite[k] * n_nodes + y
-    else:
-        slots = np.empty_like(k)
-        extra = np.zeros(k.shape)
-        flat = np.asarray(solid, dtype=bool).ravel()
-        walls = np.asarray(wall_velocity, dtype=np.float64).reshape(lattice.d, -1)
-        cw = np.asarray(lattice.c, dtype=np.float64)
-        for kk in np.unique(k):
-            sel = k == kk
-            dest = neighbour_index(y[sel], lattice.c[kk], shape)
-            blocked = flat[dest]
-            slots[sel] = np.where(blocked, opposite[kk] * n_nodes + y[sel], kk * n_nodes + dest)
-            c_dot_uw = cw[kk] @ walls[:, dest]
-            extra[sel] = 6.0 * lattice.w[kk] * c_dot_uw * blocked
-        constant += (np.asarray(values.coeff) * extra).sum(axis=1)
-    return CompiledAffine(slots=slots, coeff=np.asarray(values.coeff, dtype=np.float64), constant=constant)
+        return CompiledAffine(slots=k * n + y, coeff=coeff, constant=constant)
+    if layout == "aa_odd":
+        return CompiledAffine(slots=opp[k] * n + y, coeff=coeff, constant=constant)
+    dest = _term_destinations(lattice, k, y, shape)
+    blocked = solid.ravel()[dest]
+    slots = np.where(blocked, opp[k] * n + y, k * n + dest)
+    walls = np.asarray(wall_velocity, dtype=np.float64).reshape(lattice.d, n)
+    c = np.asarray(lattice.c, dtype=np.float64)[k]
+    cu = c[..., 0] * walls[0][dest]
+    for a in range(1, lattice.d):
+        cu = cu + c[..., a] * walls[a][dest]
+    w = np.asarray(lattice.w, dtype=np.float64)[k]
+    extra = np.where(blocked, coeff * ((6.0 * w) * cu), 0.0)
+    for t in range(extra.shape[-1]):
+        constant = constant + extra[..., t]
+    return CompiledAffine(slots=slots, coeff=coeff, constant=constant)
 
 
 def compile_targets(lattice, rules: LinkRules, layout: str, n_nodes: int) -> np.ndarray:
-    """Slot each rule writes in a pre-pass design (``link_rules.py:243-250``)."""
+    """Slot each rule's value replaces in a separate pre-pass design (the reference's GPU
+    kernels, ``link_rules.py:243-250``): the streamed population f_j(x) of the rule's link, which
+    a pull state keeps at (opp j, x) before the step and the AA states at (j, x)."""
     if layout not in LAYOUTS:
         raise ValueError(f"unknown layout {layout!r}; choose from {LAYOUTS}")
-    direction = np.asarray(rules.direction)
-    if layout == "pull":
-        direction = np.asarray(lattice.opposite)[direction]
-    return direction * n_nodes + np.asarray(rules.node)
+    j = np.asarray(rules.direction, dtype=np.int64)
+    plane = np.asarray(lattice.opposite, dtype=np.int64)[j] if layout == "pull" else j
+    return plane * n_nodes + np.asarray(rules.node, dtype=np.int64)
 
 
 def compile_rules(lattice, rules: LinkRules, layout: str, solid, wall_velocity) -> CompiledRules:

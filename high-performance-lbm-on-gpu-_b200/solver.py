@@ -884,6 +884,48 @@ class CudaSolver(Solver):
                      N.ptr(w), rows, terms, d, N.ptr(partial), N.ptr(counter), N.ptr(out), self._stream())
         return out.cpu().numpy()
 
+    def _values_on_device(self, values):
+        """Slots, coefficients and constants of an ``AffineSet`` resolved for this solver's stored
+        layout on the device (``lbm_compile_terms``: pitched slots of ``state_layout``), once per
+        set object."""
+        torch = self.torch
+        cache = self.__dict__.setdefault("_affine_cache", {})
+        key = ("values", id(values))
+        hit = cache.get(key)
+        if hit is not None and hit[0] is values:
+            return hit[1]
+        if len(cache) >= 64:
+            cache.clear()
+        to = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(self.device, dt)  # noqa: E731
+        k = to(np.asarray(values.direction, dtype=np.int64), torch.int64)
+        y = to(np.asarray(values.node, dtype=np.int64), torch.int64)
+        coeff = to(np.asarray(values.coeff, dtype=np.float64), torch.float64)
+        const = to(np.asarray(values.constant, dtype=np.float64), torch.float64)
+        rows, terms = coeff.shape if coeff.dim() == 2 else (coeff.shape[0], 1)
+        slots = torch.empty(rows * terms, dtype=torch.int64, device=self.device)
+        self._native("lbm_compile_terms", N.C.byref(self.grid), self._layout_code, None, None, rows * terms, N.ptr(k),
+                     N.ptr(y), None, N.ptr(slots), None, self._stream())
+        tensors = (slots, coeff.reshape(-1), const, (rows, terms))
+        cache[key] = (values, tensors)
+        return tensors
+
+    def reduce_affine_values(self, values, weight) -> np.ndarray:
+        """sum_r weight[r] * value_r of an uncompiled ``AffineSet`` (terms f*_k(y), natural node
+        indices), its slots resolved on the device for this solver's layout; float64 on the device."""
+        torch = self.torch
+        slots, coeff, const, (rows, terms) = self._values_on_device(values)
+        weight = np.asarray(weight, dtype=np.float64).reshape(rows, -1)
+        d = weight.shape[1]
+        if rows == 0:
+            return np.zeros(d)
+        w = torch.from_numpy(np.ascontiguousarray(weight)).to(self.device)
+        partial = torch.empty((rows + 255) // 256 * d, dtype=torch.float64, device=self.device)
+        counter = torch.zeros(1, dtype=torch.int32, device=self.device)
+        out = torch.empty(d, dtype=torch.float64, device=self.device)
+        self._native("lbm_affine_reduce", self.grid.storage, N.ptr(self._f), N.ptr(slots), N.ptr(coeff), N.ptr(const),
+                     N.ptr(w), rows, terms, d, N.ptr(partial), N.ptr(counter), N.ptr(out), self._stream())
+        return out.cpu().numpy()
+
     @property
     def immersed_force(self) -> np.ndarray:
         """Force on the immersed body during the last step, host float64 (reference ``solver.py:201-207``)."""

@@ -299,6 +299,56 @@ int lbm_affine_reduce_static(int32_t storage, const void* f, const int64_t* slot
                              const double* constant, const double* weight, int64_t n_rows, int32_t n_terms,
                              int32_t d, double* out, lbm_stream_t stream);
 
+/* ---- device-side rule compiler ------------------------------------------ */
+/* The geometry and link-rule tables of the host builders, built on the device
+ * from the solid mask (uint8 0/1, pitched like the lattice) and the body: for a
+ * 256^3 grid with a sphere the host's voxelisation and wall-link search take
+ * tens of seconds. Node indices in and out are natural (unpitched) flat
+ * indices ((z ny + y) nx + x), as the host builders use. Every floating-point
+ * operation follows the host's order with explicit IEEE rounding, so the
+ * results equal the host builders' bit for bit. A ball is its centre (cz
+ * ignored in 2D) and squared radius. */
+
+/* solid[node] = 1 at every node inside the ball -- replaces voxelize(body, shape)
+ * for a ball (src/lbm/geometry.py:140-144, 74-76). */
+int lbm_ball_voxelize(const lbm_grid_t* grid, double cx, double cy, double cz, double radius_sq, uint8_t* solid,
+                      lbm_stream_t stream);
+
+/* Every link (x, j) from a fluid node x into the ball (x - c_j inside, periodic
+ * wrap), ordered by direction j then node, with the wall fraction q along the
+ * link (first root of |x - t c_j - centre| = R, clipped to (0, 1]) -- replaces
+ * wall_links(lattice, body, solid) (src/lbm/geometry.py:174-206, 78-87).
+ * Two passes over a scratch of lbm_ball_links_scratch(grid) int64:
+ * lbm_ball_links_count leaves the link count in scratch[n - 2] and the number of
+ * nodes inside the ball that are not solid (must be 0) in scratch[n - 1];
+ * lbm_ball_links_write (same arguments and scratch) fills node[count],
+ * direction[count], q[count]. */
+int64_t lbm_ball_links_scratch(const lbm_grid_t* grid);
+int lbm_ball_links_count(const lbm_grid_t* grid, const uint8_t* solid, double cx, double cy, double cz,
+                         double radius_sq, int64_t* scratch, lbm_stream_t stream);
+int lbm_ball_links_write(const lbm_grid_t* grid, const uint8_t* solid, double cx, double cy, double cz,
+                         double radius_sq, const int64_t* scratch, int64_t* node, int32_t* direction, double* q,
+                         lbm_stream_t stream);
+
+/* The Bouzidi rule of each link -- replaces bouzidi_rules (src/lbm/link_rules.py:154-188):
+ * with i = opp(j), link r gets two terms (term_dir/term_node/coeff[2r], [2r + 1]):
+ * q < 1/2: 2q f*_i(x) + (1 - 2q) f*_i(x + c_j); q >= 1/2: f*_i(x)/(2q) + (1 - 1/(2q)) f*_j(x);
+ * keep[r] = 0 where q < 1/2 and x + c_j is solid (the link keeps plain bounce-back). */
+int lbm_bouzidi_links(const lbm_grid_t* grid, const uint8_t* solid, int64_t n, const int64_t* node,
+                      const int32_t* direction, const double* q, uint8_t* keep, int64_t* term_dir,
+                      int64_t* term_node, double* coeff, lbm_stream_t stream);
+
+/* Slots of affine terms f*_k(y) in a stored layout, pitched for this library's
+ * buffers (slot = direction plane * qstride + pitched node) -- replaces the slot
+ * resolution of compile_affine (src/lbm/link_rules.py:203-240): LBM_LAYOUT_PULL
+ * (k, y); LBM_LAYOUT_AA_ODD (opp k, y); LBM_LAYOUT_AA_EVEN (k, y + c_k), or
+ * (opp k, y) where y + c_k is solid, with extra[t] = coeff[t] 6 w_k (c_k . u_w(y + c_k))
+ * (wall_u: float64 (d, qstride) pitched, or NULL: extra is 0) to add to the row's
+ * constant. solid is needed for LBM_LAYOUT_AA_EVEN only; extra may be NULL. */
+int lbm_compile_terms(const lbm_grid_t* grid, int32_t layout, const uint8_t* solid, const double* wall_u, int64_t n,
+                      const int64_t* direction, const int64_t* node, const double* coeff, int64_t* slot,
+                      double* extra, lbm_stream_t stream);
+
 /* ---- immersed boundary (direct forcing, multi-direct) ------------------- */
 /* Replaces ImmersedForcing.force_field (src/lbm/ibm.py:189-214). */
 

@@ -14,6 +14,7 @@ from tests import cases
 from tests.helpers import NS, assert_rules_match, golden
 
 import lbm_b200 as lbm
+from oracle import reference_package
 
 
 @pytest.mark.parametrize("d", [2, 3])
@@ -189,3 +190,36 @@ def test_rules_compile_to_the_reference_prepass_slots(d, case, layout):
         assert terms.keys() == terms2.keys(), t
         for slot, a in terms.items():
             assert abs(a - terms2[slot]) <= 1e-15, (t, slot)
+
+
+@pytest.mark.skipif(not reference_package.available(), reason="baseline/_ref is absent")
+@pytest.mark.parametrize("case", ["bouzidi2", "bouzidi3", "plain_moving", "cylinder"])
+def test_force_probe_rows_equal_the_reference_builders(case):
+    """ForceProbe.build (vectorised) gives the reference's rows term for term, for links with
+    rules, links with plain bounce-back next to a moving wall, and the cylinder configuration."""
+    from tests.helpers import reference_ns
+
+    ref_ns = reference_ns()
+    from lbm.forces import ForceProbe as RefProbe  # noqa: PLC0415
+
+    def build(ns):
+        if case.startswith("bouzidi"):
+            return cases.bouzidi(ns, int(case[-1]), "float64")
+        if case == "cylinder":
+            p, links, _ = cases.cylinder_channel(ns, "bouzidi", dtype="float64")
+            return p, links
+        # plain bounce-back links into a body next to a moving lid (no rules)
+        solid, wall = ns.cavity_walls(20, 0.05)
+        body = ns.circle(10.2, 17.9, 3.1)
+        solid = solid | ns.voxelize(body, solid.shape)
+        links = ns.wall_links(ns.default_lattice(2), body, solid)
+        return ns.SimulationParams(nx=22, ny=22, tau=0.7, solid=solid, wall_velocity=wall), links
+
+    p, links = build(NS)
+    rp, rlinks = build(ref_ns)
+    ours, theirs = lbm.ForceProbe.build(p, links), RefProbe.build(rp, rlinks)
+    np.testing.assert_array_equal(ours.weight, theirs.weight)
+    np.testing.assert_array_equal(ours.values.direction, theirs.values.direction)
+    np.testing.assert_array_equal(ours.values.node, theirs.values.node)
+    np.testing.assert_allclose(ours.values.coeff, theirs.values.coeff, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(ours.values.constant, theirs.values.constant, rtol=0, atol=1e-15)
