@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -81,7 +81,7 @@ class Ibm(C.Structure):
     _fields_ = [
         ("n_nodes", i32), ("n_markers", i32), ("stencil_size", i32), ("node", vp), ("stencil", vp),
         ("weight", vp), ("area", vp), ("inv_start", vp), ("inv_marker", vp), ("inv_weight", vp),
-        ("rho", vp), ("u_star", vp), ("marker_force", vp),
+        ("rho", vp), ("u_star", vp), ("marker_force", vp), ("marker_scratch", vp),
     ]
 
 

@@ -132,11 +132,13 @@ class AdjointRun:
             "force": torch.zeros((tab.iterations, d, n), dtype=real, device=dev),
             "adj": [torch.zeros((d, n), dtype=real, device=dev) for _ in range(2)],
             "moments": torch.zeros((1 + d, n), dtype=torch.float64, device=dev),
+            # each marker's forward and adjoint terms of a reverse pass, formed once
+            "marker_scratch": torch.zeros((1 + 2 * d, tab.n_markers), dtype=torch.float64, device=dev),
         }
         base = ibm.struct
         st["struct"] = N.Ibm(base.n_nodes, base.n_markers, base.stencil_size, base.node, base.stencil, base.weight,
                              base.area, base.inv_start, base.inv_marker, base.inv_weight, N.ptr(st["rho"]),
-                             N.ptr(st["u_star"]), N.ptr(st["marker_force"]))
+                             N.ptr(st["u_star"]), N.ptr(st["marker_force"]), N.ptr(st["marker_scratch"]))
         return st
 
     def _ibm_recompute(self, f, stream):

@@ -176,4 +176,4 @@ extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t wh
 
 extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
 
-extern "C" int32_t lbm_abi_version(void) { return 6; }
+extern "C" int32_t lbm_abi_version(void) { return 7; }

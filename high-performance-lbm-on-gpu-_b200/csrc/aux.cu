@@ -246,17 +246,25 @@ __global__ void health_kernel(const lbm_grid_t g, const uint8_t* __restrict__ ki
     if (any_nf && (threadIdx.x & 31) == 0) atomicMax((unsigned long long*)(out + 1), 1ull);
 }
 
-// Sum of the checked step's per-block partials in a fixed order: 256 threads
-// each add a strided subset in index order, then a fixed tree.
-__global__ void __launch_bounds__(256) health_finish_kernel(const double* __restrict__ partial, int64_t n,
-                                                            double* __restrict__ out)
+// Sum of the checked step's per-block partials in a fixed order: 1024
+// threads each add a strided subset in index order (four independent
+// accumulators, combined in order), then a fixed tree.
+__global__ void __launch_bounds__(1024) health_finish_kernel(const double* __restrict__ partial, int64_t n,
+                                                             double* __restrict__ out)
 {
-    __shared__ double sums[256];
-    double s = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += 256) s += partial[i];
-    sums[threadIdx.x] = s;
+    __shared__ double sums[1024];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int64_t i = threadIdx.x;
+    for (; i + 3 * 1024 < n; i += 4 * 1024) {
+        s0 += partial[i];
+        s1 += partial[i + 1024];
+        s2 += partial[i + 2 * 1024];
+        s3 += partial[i + 3 * 1024];
+    }
+    for (; i < n; i += 1024) s0 += partial[i];
+    sums[threadIdx.x] = (s0 + s1) + (s2 + s3);
     __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
+    for (int w = 512; w > 0; w >>= 1) {
         if ((int)threadIdx.x < w) sums[threadIdx.x] += sums[threadIdx.x + w];
         __syncthreads();
     }
@@ -421,7 +429,7 @@ extern "C" int lbm_health_reset(int64_t* out, lbm_stream_t stream)
 extern "C" int lbm_health_finish(const lbm_health_t* h, double* delta_mass, lbm_stream_t stream)
 {
     if (!h || !h->partial || h->n_partial <= 0 || !delta_mass) return LBM_ERR_INVALID;
-    health_finish_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(h->partial, h->n_partial, delta_mass);
+    health_finish_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(h->partial, h->n_partial, delta_mass);
     return launch_status();
 }
 

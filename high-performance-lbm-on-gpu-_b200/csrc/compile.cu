@@ -123,33 +123,49 @@ __global__ void __launch_bounds__(COMPILE_THREADS) ball_links_count_kernel(const
     if (threadIdx.x < L::Q) offs[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = counts[threadIdx.x];
 }
 
-// Exclusive scan of offs[0 .. n) in place, total into offs[n]: one block,
-// each thread a contiguous chunk, then the chunk sums in order.
+// Exclusive scan of offs[0 .. n) in place, total into offs[n]: one block of
+// 32 warps. Warp w scans the contiguous segment [w n/32, (w + 1) n/32) in
+// coalesced runs of 32 (a shuffle scan per run, carrying the running total);
+// the warp totals are then scanned in order and added back.
+__device__ __forceinline__ int64_t warp_inclusive_scan(int64_t v, int lane)
+{
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int64_t u = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += u;
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(1024) exclusive_scan_kernel(int64_t* __restrict__ offs, int64_t n)
 {
-    __shared__ int64_t sums[1024];
-    const int64_t chunk = (n + 1023) / 1024;
-    const int64_t lo = threadIdx.x * chunk, hi = lo + chunk < n ? lo + chunk : n;
-    int64_t s = 0;
-    for (int64_t i = lo; i < hi; ++i) s += offs[i];
-    sums[threadIdx.x] = s;
+    __shared__ int64_t warp_total[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t seg = (n + 31) / 32;
+    const int64_t lo = warp * seg, hi = lo + seg < n ? lo + seg : n;
+    int64_t carry = 0;
+    for (int64_t base = lo; base < hi; base += 32) {
+        const int64_t i = base + lane;
+        const int64_t v = i < hi ? offs[i] : 0;
+        const int64_t inc = warp_inclusive_scan(v, lane);
+        if (i < hi) offs[i] = carry + inc - v;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) warp_total[warp] = carry;
     __syncthreads();
     if (threadIdx.x == 0) {
         int64_t run = 0;
-        for (int t = 0; t < 1024; ++t) {
-            const int64_t v = sums[t];
-            sums[t] = run;
+        for (int w = 0; w < 32; ++w) {
+            const int64_t v = warp_total[w];
+            warp_total[w] = run;
             run += v;
         }
         offs[n] = run;
     }
     __syncthreads();
-    int64_t run = sums[threadIdx.x];
-    for (int64_t i = lo; i < hi; ++i) {
-        const int64_t v = offs[i];
-        offs[i] = run;
-        run += v;
-    }
+    const int64_t add = warp_total[warp];
+    if (add != 0)
+        for (int64_t i = lo + lane; i < hi; i += 32) offs[i] += add;
 }
 
 // Pass 2: the links of direction j of this block go to offs[j * blocks + block]

@@ -288,6 +288,82 @@ __global__ void ibm_iteration_kernel(const lbm_ibm_t ib, int iteration, const ty
     }
 }
 
+// The per-pass path of large bodies in two launches, marker-centric then
+// node-centric, so that no marker is recomputed: ibm_markers_kernel forms F_l
+// of every marker once (the operations of ibm_iteration_kernel, in its order)
+// into marker_force[iteration], ibm_spread_kernel adds w_ln F_l over each
+// node's CSR list in float64. Same bits as the one-kernel pass.
+template <class L, int ST>
+__global__ void __launch_bounds__(128) ibm_markers_kernel(const lbm_ibm_t ib, int iteration,
+                                                          const typename Storage<ST>::R* __restrict__ fin)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    constexpr int S = D == 2 ? 9 : 27;
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= ib.n_markers) return;
+    const int nn = ib.n_nodes;
+    const R* __restrict__ rho = (const R*)ib.rho;
+    const R* __restrict__ us = (const R*)ib.u_star;
+    const int* st = ib.stencil + (int64_t)l * S;
+    const R* wl = (const R*)ib.weight + (int64_t)l * S;
+    int m[S];
+    R w[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        m[s] = st[s];
+        w[s] = wl[s];
+    }
+    R rho_l = R(0);
+    R U[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) U[a] = R(0);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const R rm = rho[m[s]];
+        rho_l += w[s] * rm;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            R u = us[a * nn + m[s]];
+            if (fin != nullptr) u += fin[a * nn + m[s]] / (R(2) * rm);
+            U[a] += w[s] * u;
+        }
+    }
+    R* mf = (R*)ib.marker_force + (int64_t)iteration * D * ib.n_markers;
+    const R ar = ((const R*)ib.area)[l];
+#pragma unroll
+    for (int a = 0; a < D; ++a) mf[(int64_t)a * ib.n_markers + l] = R(2) * rho_l * (R(0) - U[a]) * ar;
+}
+
+template <class L, int ST>
+__global__ void __launch_bounds__(128) ibm_spread_kernel(const lbm_ibm_t ib, int iteration,
+                                                         const typename Storage<ST>::R* __restrict__ fin,
+                                                         typename Storage<ST>::R* __restrict__ fout)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ib.n_nodes) return;
+    const int nn = ib.n_nodes, nm = ib.n_markers;
+    const R* __restrict__ mf = (const R*)ib.marker_force + (int64_t)iteration * D * nm;
+    const R* __restrict__ invw = (const R*)ib.inv_weight;
+    double acc[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) acc[a] = 0.0;
+    const int q1 = ib.inv_start[n + 1];
+    for (int q = ib.inv_start[n]; q < q1; ++q) {
+        const int l = ib.inv_marker[q];
+        const R wn = invw[q];
+#pragma unroll
+        for (int a = 0; a < D; ++a) acc[a] += (double)(wn * mf[(int64_t)a * nm + l]);
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const double base = fin != nullptr ? (double)fin[a * nn + n] : 0.0;
+        fout[a * nn + n] = (R)(base + acc[a]);
+    }
+}
+
 // Body force -sum over passes and markers, one block, fixed order.
 template <class L, int ST>
 __global__ void ibm_body_force_kernel(const lbm_ibm_t ib, int iterations, double* out)
@@ -383,6 +459,108 @@ __global__ void ibm_adjoint_iteration_kernel(const lbm_ibm_t ib, const typename 
     for (int a = 0; a < D; ++a) madj[(int64_t)(1 + a) * nn + n] += ub[a];
 }
 
+// The adjoint pass in two launches when the caller gives marker scratch
+// (lbm_ibm_t.marker_scratch, (1 + 2 d) doubles per marker): the forward rho_l
+// and U_l and the adjoint Fbar_l of each marker once, then the node-centric
+// accumulation of ibm_adjoint_iteration_kernel reading them -- the same values
+// in the same order, so the same bits, without recomputing each marker for
+// every one of its 3^d nodes.
+template <class L, int ST>
+__global__ void __launch_bounds__(128) ibm_adjoint_markers_kernel(const lbm_ibm_t ib,
+                                                                  const typename Storage<ST>::R* __restrict__ fprev,
+                                                                  const typename Storage<ST>::R* __restrict__ adj_in,
+                                                                  int axis, double body_scale)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    constexpr int S = D == 2 ? 9 : 27;
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= ib.n_markers) return;
+    const int nn = ib.n_nodes, nm = ib.n_markers;
+    const R* __restrict__ rho = (const R*)ib.rho;
+    const R* __restrict__ us = (const R*)ib.u_star;
+    const int* st = ib.stencil + (int64_t)l * S;
+    const R* wl = (const R*)ib.weight + (int64_t)l * S;
+    int m[S];
+    double w[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        m[s] = st[s];
+        w[s] = (double)wl[s];
+    }
+    double rho_l = 0.0, U[D], Fb[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) U[a] = Fb[a] = 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const double rm = (double)rho[m[s]];
+        rho_l += w[s] * rm;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            double u = (double)us[a * nn + m[s]];
+            if (fprev != nullptr) u += (double)fprev[a * nn + m[s]] / (2.0 * rm);
+            U[a] += w[s] * u;
+            Fb[a] += w[s] * (double)adj_in[a * nn + m[s]];
+        }
+    }
+    if (axis >= 0 && axis < D) Fb[axis] -= body_scale;
+    double* sc = ib.marker_scratch;
+    sc[l] = rho_l;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        sc[(int64_t)(1 + a) * nm + l] = U[a];
+        sc[(int64_t)(1 + D + a) * nm + l] = Fb[a];
+    }
+}
+
+template <class L, int ST>
+__global__ void __launch_bounds__(128) ibm_adjoint_nodes_kernel(const lbm_ibm_t ib,
+                                                                const typename Storage<ST>::R* __restrict__ fprev,
+                                                                const typename Storage<ST>::R* __restrict__ adj_in,
+                                                                typename Storage<ST>::R* __restrict__ adj_out,
+                                                                double* __restrict__ madj)
+{
+    using R = typename Storage<ST>::R;
+    constexpr int D = L::D;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ib.n_nodes) return;
+    const int nn = ib.n_nodes, nm = ib.n_markers;
+    const R* __restrict__ area = (const R*)ib.area;
+    const R* __restrict__ invw = (const R*)ib.inv_weight;
+    const double* __restrict__ sc = ib.marker_scratch;
+    const double rho_n = (double)((const R*)ib.rho)[n];
+    double fp[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) fp[a] = fprev != nullptr ? (double)fprev[a * nn + n] : 0.0;
+    double o[D], ub[D], rb = 0.0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) o[a] = ub[a] = 0.0;
+    const int q1 = ib.inv_start[n + 1];
+    for (int q = ib.inv_start[n]; q < q1; ++q) {
+        const int l = ib.inv_marker[q];
+        const double rho_l = sc[l];
+        const double wn = (double)invw[q], dA = (double)area[l];
+        const double c = dA * rho_l * wn;
+        double UF = 0.0, PF = 0.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const double U = sc[(int64_t)(1 + a) * nm + l], Fb = sc[(int64_t)(1 + D + a) * nm + l];
+            o[a] += c * Fb;
+            ub[a] -= 2.0 * c * Fb;
+            UF += U * Fb;
+            if (fprev != nullptr) PF += Fb * fp[a];
+        }
+        rb += -2.0 * dA * wn * UF + c * PF / (rho_n * rho_n);
+    }
+    if (adj_out != nullptr) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) adj_out[a * nn + n] = (R)((double)adj_in[a * nn + n] - o[a] / rho_n);
+    }
+    madj[n] += rb;
+#pragma unroll
+    for (int a = 0; a < D; ++a) madj[(int64_t)(1 + a) * nn + n] += ub[a];
+}
+
 // rho = 1 + sum_k s_k, u* = (j + F_uniform / 2) / rho, j = sum_k c_k s_k:
 //   d/ds_k = rho_bar - u*_bar . u* / rho + c_k . u*_bar / rho
 template <class L, int ST>
@@ -419,6 +597,14 @@ int ibm_adjoint_iteration(const lbm_grid_t& g, const lbm_ibm_t& ib, const void* 
 {
     using R = typename Storage<ST>::R;
     if (ib.n_nodes <= 0) return LBM_OK;
+    if (ib.marker_scratch != nullptr) {
+        if (ib.n_markers > 0)
+            ibm_adjoint_markers_kernel<L, ST><<<blocks_for(ib.n_markers, 128), 128, 0, s>>>(
+                ib, (const R*)fprev, (const R*)adj_in, axis, body_scale);
+        ibm_adjoint_nodes_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(ib, (const R*)fprev,
+                                                                                  (const R*)adj_in, (R*)adj_out, madj);
+        return launch_status();
+    }
     ibm_adjoint_iteration_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(
         ib, (const R*)fprev, (const R*)adj_in, axis, body_scale, (R*)adj_out, madj);
     return launch_status();
@@ -468,9 +654,11 @@ int ibm_force(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, 
     }
     ibm_moments_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(g, p, ib, (const T*)f, layout);
     const int64_t plane = (int64_t)L::D * ib.n_nodes;
-    for (int it = 0; it < iterations; ++it)
-        ibm_iteration_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(
-            ib, it, it == 0 ? nullptr : out + (it - 1) * plane, out + it * plane);
+    for (int it = 0; it < iterations; ++it) {
+        const R* fin = it == 0 ? nullptr : out + (it - 1) * plane;
+        if (ib.n_markers > 0) ibm_markers_kernel<L, ST><<<blocks_for(ib.n_markers, 128), 128, 0, s>>>(ib, it, fin);
+        ibm_spread_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(ib, it, fin, out + it * plane);
+    }
     return launch_status();
 }
 
@@ -479,7 +667,9 @@ int ibm_iteration(const lbm_grid_t& g, const lbm_ibm_t& ib, int iteration, const
 {
     using R = typename Storage<ST>::R;
     if (ib.n_nodes <= 0) return LBM_OK;
-    ibm_iteration_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(ib, iteration, (const R*)fin, (R*)fout);
+    if (ib.n_markers > 0)
+        ibm_markers_kernel<L, ST><<<blocks_for(ib.n_markers, 128), 128, 0, s>>>(ib, iteration, (const R*)fin);
+    ibm_spread_kernel<L, ST><<<blocks_for(ib.n_nodes, 128), 128, 0, s>>>(ib, iteration, (const R*)fin, (R*)fout);
     return launch_status();
 }
 

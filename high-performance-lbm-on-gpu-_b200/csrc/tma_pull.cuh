@@ -98,6 +98,22 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+// Bulk tensor store of a shared-memory tile (x must be a multiple of 8 nodes
+// for 16-bit data; every store here starts at x = 0 and y, z >= 0).
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void* src, int x, int y, int z, int w)
+{
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];"
+                 ::"l"(map), "r"(smem_addr(src)), "r"(x), "r"(y), "r"(z), "r"(w)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// The committed stores have finished reading shared memory ...
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... and have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Shared-memory writes of this thread become visible to the bulk-copy (async) proxy.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 template <class L>
 __host__ __device__ constexpr uint32_t tma_pop_bytes(int nx)
 {
@@ -107,6 +123,17 @@ template <class L>
 __host__ __device__ constexpr uint32_t tma_stage_bytes(int nx)
 {
     return (tma_pop_bytes<L>(nx) + TMA_ROWS * (uint32_t)nx + 127u) & ~127u;
+}
+// The odd AA half's output buffer (one tile of populations; a multiple of 128 bytes).
+template <class L, int VAR>
+__host__ __device__ constexpr uint32_t tma_out_bytes(int nx)
+{
+    return VAR == LBM_AA_ODD ? tma_pop_bytes<L>(nx) : 0u;
+}
+template <class L, int VAR>
+__host__ __device__ constexpr uint32_t tma_smem_bytes(int nx)
+{
+    return TMA_STAGES * tma_stage_bytes<L>(nx) + tma_out_bytes<L, VAR>(nx) + 8u * TMA_STAGES;
 }
 
 // Halfway bounce-back on the staged path: each link i whose source x - c_i
@@ -136,6 +163,68 @@ __device__ __forceinline__ void bounce(const StepArgs& a, typename Storage<ST>::
 #pragma unroll
         for (int j = 1; j < L::Q; ++j)
             if (j == i) f[j] = v;
+    }
+}
+
+// The streamed populations of pair (x0, x0 + 1) from a staged row set (the
+// odd AA half and the pull: direction i's row at st_row + i * plane, staged
+// from the source rows y - c_y, z - c_z; x - c_x read in the row, wrapped).
+template <class L, int ST>
+__device__ __forceinline__ void staged_gather(const typename Storage<ST>::T* st_row, int plane, int x0, int nx,
+                                              typename Storage<ST>::R (&fa)[L::Q], typename Storage<ST>::R (&fb)[L::Q])
+{
+    using S = Storage<ST>;
+    const int xm = x0 == 0 ? nx - 1 : x0 - 1;  // x0 - 1, wrapped
+    const int xp = x0 + 2 == nx ? 0 : x0 + 2;  // x0 + 2, wrapped
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        const unsigned short* row = reinterpret_cast<const unsigned short*>(st_row + i * plane);
+        if (L::cx(i) == 0) {
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(row + x0);
+            fa[i] = S::decode_lo(w);
+            fb[i] = S::decode_hi(w);
+        } else if (L::cx(i) > 0) {  // sources x0 - 1, x0
+            fa[i] = S::decode_lo(row[xm]);
+            fb[i] = S::decode_lo(row[x0]);
+        } else {  // sources x0 + 1, x0 + 2
+            fa[i] = S::decode_lo(row[x0 + 1]);
+            fb[i] = S::decode_lo(row[xp]);
+        }
+    }
+}
+
+// Odd AA half of an interior pair, outputs staged for bulk stores: out_row is
+// direction 0's row of the tile's output buffer (direction i at out_row + i *
+// plane), holding in destination order the values that the whole rows y + c_y,
+// z + c_z of slot i receive: node x pushes f*_i to x + c_x (wrapped in the row).
+template <class L, int ST>
+__device__ __forceinline__ void tma_aa_odd_staged(const StepArgs& a, const typename Storage<ST>::T* st_row, int plane,
+                                                  unsigned short* out_row, int x0, int y, int z,
+                                                  const Relax<typename Storage<ST>::R>& rc, uint32_t t_seed)
+{
+    using S = Storage<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q;
+    const int nx = a.nx;
+    R fa[Q], fb[Q];
+    staged_gather<L, ST>(st_row, plane, x0, nx, fa, fb);
+    collide_pair<L, S::SCALE_LOG2>(fa, fb, rc, R(a.fx), R(a.fy), R(a.fz));
+    const uint32_t h = sr_pair_hash(sr_pair(nx, a.ny, x0, y, z), t_seed);
+    const int xm = x0 == 0 ? nx - 1 : x0 - 1;
+    const int xp = x0 + 2 == nx ? 0 : x0 + 2;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const uint32_t w = S::pack_sr(fa[i], fb[i], sr_word(h, i));  // (x0, x0 + 1) rounded
+        unsigned short* o = out_row + i * plane;
+        if (L::cx(i) == 0) {
+            *reinterpret_cast<uint32_t*>(o + x0) = w;
+        } else if (L::cx(i) > 0) {  // x0 -> x0 + 1, x0 + 1 -> x0 + 2
+            o[x0 + 1] = (unsigned short)w;
+            o[xp] = (unsigned short)(w >> 16);
+        } else {  // x0 -> x0 - 1, x0 + 1 -> x0
+            o[xm] = (unsigned short)w;
+            o[x0] = (unsigned short)(w >> 16);
+        }
     }
 }
 
@@ -276,7 +365,9 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
     const uint32_t stage_bytes = tma_stage_bytes<L>(nx);
     const int plane = H * nx;  // populations per staged direction
     const int log_half = __ffs(nx) - 2;  // log2(nx / 2)
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + TMA_STAGES * stage_bytes);
+    // the odd AA half stages its outputs for bulk stores in a buffer after the stages
+    unsigned short* out = reinterpret_cast<unsigned short*>(smem + TMA_STAGES * stage_bytes);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + TMA_STAGES * stage_bytes + tma_out_bytes<L, VAR>(nx));
     const int tid = threadIdx.x;
 
     advance_seed(a);
@@ -356,8 +447,41 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
         issued &= ~(1u << s);
         const T* st = reinterpret_cast<const T*>(smem + s * stage_bytes);
         const unsigned char* kinds = smem + s * stage_bytes + pop_bytes;
+        bool staged_out = false;
+        if constexpr (VAR == LBM_AA_ODD) {
+            // A tile of interior nodes only (kinds 0 and EDGE, rows off the y and z faces):
+            // outputs into the buffer in destination order, then one bulk store per direction
+            // of the whole rows y0 + c_y, z + c_z of slot i (every slot of them comes from this
+            // tile: x wraps inside the row, and no push meets a wall).
+            bool ok = true;
+            for (int p = tid; p < plane / 2; p += TMA_THREADS) {
+                const int r = p >> log_half;
+                const int x0 = 2 * (p - (r << log_half));
+                const int y = y0 + r;
+                const uint32_t k2 = *reinterpret_cast<const unsigned short*>(kinds + r * nx + x0);
+                ok = ok && y >= 1 && y <= ny - 2 && (L::D == 2 || (z >= 1 && z <= nz - 2)) && (k2 & ~0x0808u) == 0u;
+            }
+            if (__syncthreads_and(ok)) {
+                if (tid == 0) bulk_wait_read();  // the previous tile's stores have read the buffer
+                __syncthreads();
 #pragma unroll 1
-        for (int p = tid; p < plane / 2; p += TMA_THREADS) {
+                for (int p = tid; p < plane / 2; p += TMA_THREADS) {
+                    const int r = p >> log_half;
+                    const int x0 = 2 * (p - (r << log_half));
+                    tma_aa_odd_staged<L, ST>(a, st + r * nx, plane, out + r * nx, x0, y0 + r, z, rc, t_seed);
+                }
+                fence_proxy_async();
+                __syncthreads();
+                if (tid == 0) {
+#pragma unroll
+                    for (int i = 0; i < Q; ++i) tma_store_4d(&map, out + i * plane, 0, y0 + L::cy(i), z + L::cz(i), i);
+                    bulk_commit();
+                }
+                staged_out = true;
+            }
+        }
+#pragma unroll 1
+        for (int p = staged_out ? plane / 2 : tid; p < plane / 2; p += TMA_THREADS) {
             const int r = p >> log_half;
             const int x0 = 2 * (p - (r << log_half));
             const int y = y0 + r;
@@ -425,6 +549,10 @@ __device__ __forceinline__ void tma_step(const CUtensorMap& map, const CUtensorM
         for (int k = 0; k < TMA_STAGES; ++k)
             if ((issued >> k) & 1u) mbar_wait(&bar[k], (phases >> k) & 1u, WAIT_LIMIT_DEFAULT);
     }
+    // no bulk store may still read shared memory when the block exits
+    if constexpr (VAR == LBM_AA_ODD) {
+        if (tid == 0) bulk_wait_all();
+    }
 }
 
 template <class L, int ST>
@@ -435,8 +563,13 @@ __global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_pull_k
     tma_step<L, ST, LBM_PULL>(map, kmap, a, status);
 }
 
+// The odd AA half holds a third buffer of shared memory (its staged outputs),
+// so three blocks fit on an SM, not five: its register bound follows.
+template <int VAR>
+constexpr int tma_min_blocks() { return VAR == LBM_AA_ODD ? 3 : TMA_BLOCKS_PER_SM; }
+
 template <class L, int ST, int VAR>
-__global__ void __launch_bounds__(TMA_THREADS, TMA_BLOCKS_PER_SM) lbm_tma_aa_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(TMA_THREADS, tma_min_blocks<VAR>()) lbm_tma_aa_kernel(const __grid_constant__ CUtensorMap map,
                                                                     const __grid_constant__ CUtensorMap kmap,
                                                                     const StepArgs a, uint32_t* status)
 {
@@ -510,7 +643,7 @@ bool launch_tma(const StepArgs& a, cudaStream_t stream, int* status_out)
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
-    const size_t smem = TMA_STAGES * (size_t)tma_stage_bytes<L>(a.nx) + 8 * TMA_STAGES;
+    const size_t smem = tma_smem_bytes<L, VAR>(a.nx);
     int device = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) {
         cudaGetLastError();
@@ -522,7 +655,7 @@ bool launch_tma(const StepArgs& a, cudaStream_t stream, int* status_out)
     const unsigned long long ctx = current_context_id();
     if (ctx == 0 || configured[device] != ctx) {
         if (cudaFuncSetAttribute(tma_kernel<L, ST, VAR>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(TMA_STAGES * tma_stage_bytes<L>(256) + 8 * TMA_STAGES)) != cudaSuccess) {
+                                 (int)tma_smem_bytes<L, VAR>(256)) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }

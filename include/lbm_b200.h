@@ -368,6 +368,9 @@ typedef struct lbm_ibm {
     void* rho;                 /* real[n_nodes] scratch */
     void* u_star;              /* real[d][n_nodes] scratch */
     void* marker_force;        /* real[iterations][d][n_markers]: F_l of every pass */
+    double* marker_scratch;    /* (1 + 2 d) doubles per marker for lbm_ibm_adjoint_iteration (each marker's
+                                  terms formed once, then read by its nodes), or NULL (each node forms the
+                                  terms of its markers itself); same results either way */
 } lbm_ibm_t;
 
 /* Moments of the streamed populations at the stencil nodes (state in layout). */
@@ -375,7 +378,9 @@ int lbm_ibm_moments(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm
                     const void* f, int32_t layout, lbm_stream_t stream);
 
 /* One multi-direct pass: force_out = force_in + spread of the marker forces
- * computed from u* + force_in / (2 rho). force_in may be NULL (first pass). */
+ * computed from u* + force_in / (2 rho). force_in may be NULL (first pass).
+ * Two launches: the marker forces (into marker_force[iteration]), then the
+ * node-centric spread. */
 int lbm_ibm_iteration(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iteration,
                       const void* force_in, void* force_out, lbm_stream_t stream);
 
