@@ -76,15 +76,23 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched-cavities study (aggregate MLUPS against separate launches)")
-    ap.add_argument("--study", choices=("tgv", "cylinder", "batched", "adjoint", "precision", "setup"), default=None,
+    ap.add_argument("--study", choices=("tgv", "cylinder", "batched", "adjoint", "precision", "setup", "kernels"),
+                    default=None,
                     help="run one configuration study alone and print its JSON (no duct line)")
     ap.add_argument("--study-steps", type=int, default=None, help="steps of --study (default: the study's own)")
+    ap.add_argument("--cylinder-method", choices=("both", "bouzidi", "ibm"), default="both",
+                    help="body of --study cylinder")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the Taylor-Green and cylinder configuration studies")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the adjoint-configuration study (forward/backward cost and finite differences)")
     ap.add_argument("--precision-steps", type=int, default=5000,
                     help="steps of the storage-precision study (0 = skip)")
+    ap.add_argument("--repeat-seconds", type=float, default=MIN_TIMED_SECONDS,
+                    help="repeat the timed region of exactly --steps steps until the repeats span this long "
+                         "(at least 3 repeats); 0 for three repeats (profiling)")
+    ap.add_argument("--no-run-loop", dest="run_loop", action="store_false",
+                    help="skip the public run-loop measurement (fused state checks)")
     return ap.parse_args()
 
 
@@ -479,14 +487,14 @@ def cylinder_params(lbm, method: str, nx: int = 880, ny: int = 164, u_max: float
     return params, links, u_mean
 
 
-def cylinder_study(lbm, torch, steps: int = 40000, every: int = 100):
+def cylinder_study(lbm, torch, steps: int = 40000, every: int = 100, methods=("bouzidi", "ibm")):
     """Cylinder configuration, Bouzidi and immersed boundary: `steps` steps from rest through the public run
     loop, drag and lift sampled every `every` steps in float64 (force probe / immersed-body force), as
     C = F / (0.5 U_mean^2 D). MLUPS of the whole run (wall clock, samples included) and of the steps alone
     (CUDA events, no sampling); C_D mean and C_L range over the last quarter of the run.
     """
     out = {}
-    for method in ("bouzidi", "ibm"):
+    for method in methods:
         params, links, u_mean = cylinder_params(lbm, method)
         s = lbm.make_solver(params, backend="cuda-naive")
         probe = lbm.ForceProbe.build(params, links) if links is not None else None
@@ -600,6 +608,85 @@ def setup_study(lbm, torch):
     return out
 
 
+def kernels_study(lbm, torch):
+    """Every kernel family outside the headline step, each launched a few times on a small case
+    whose inputs exceed L2 (a few hundred MB on the device), timed with CUDA events: the driver of
+    the per-family ncu launch list (``ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,
+    dram__bytes_write.sum``). Families: the 16-bit node-pair fallbacks (nx = 200, pull and AA);
+    on a 192^3 float32 duct the checked step (state check fused), the separate scan, the
+    macroscopic readout and the regularised step; the per-pass immersed boundary of a large body
+    (sphere r = 20, 5 027 markers); the immersed-body adjoint (3D channel); the device-side rule
+    compiler on a 256^3 duct with a sphere of radius 40."""
+    import dataclasses
+
+    from lbm_b200 import _native as N
+    from lbm_b200 import device_rules
+    from lbm_b200.adjoint import AdjointRun
+    from tests import cases
+    from tests.helpers import NS
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, n=5):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(n):
+            fn()
+        ev[1].record()
+        ev[1].synchronize()
+        return round(ev[0].elapsed_time(ev[1]) / n * 1e3, 1)
+
+    out = {}
+    for backend in ("cuda-naive", "cuda-aa"):
+        s = lbm.make_solver(cases.duct(NS, n=128, nx=200, dtype="float16"), backend=backend, graph=False)
+        out[f"float16_pair_kernel_{backend}_us_per_step"] = timed(lambda: s._advance(2)) / 2
+        del s
+    p = cases.duct(NS, n=192, dtype="float32")
+    s = lbm.make_solver(p, backend="cuda-naive", graph=False)
+    out["checked_step_us"] = timed(lambda: s._advance_checked(1))
+    def scan():
+        s._health_fresh = False  # the separate scan, as after a state set from outside the run loop
+        s._check_health()
+
+    out["health_scan_us"] = timed(scan)
+    out["macroscopic_ms"] = timed(lambda: s.macroscopic()) / 1e3
+    del s
+    s = lbm.make_solver(dataclasses.replace(p, collision="regularized"), backend="cuda-naive", graph=False)
+    out["regularized_step_us"] = timed(lambda: s._advance(1))
+    del s
+    torch.cuda.empty_cache()
+    solid = lbm.duct_walls(96, 64, 64)
+    body = lbm.ImmersedBoundary.from_ball(lbm.sphere(40.0, 31.5, 31.5, 20.0), spacing=1.0, iterations=3)
+    p = lbm.SimulationParams(nx=96, ny=64, nz=64, tau=0.7, collision="trt", solid=solid, force=(1e-6, 0, 0),
+                             immersed=body)
+    s = lbm.make_solver(p, backend="cuda-naive", graph=False)
+    out["ibm_large_body"] = {"markers": int(s._ibm.tables.n_markers), "nodes": int(s._ibm.tables.n_nodes),
+                             "force_us": timed(lambda: s._ibm.run(s._f, N.LAYOUT_PULL)),
+                             "step_us": timed(lambda: s._advance(1))}
+    del s
+    # immersed sphere in a Zou-He duct channel, loss = the body's drag
+    lat, solid = lbm.D3Q19, lbm.duct_walls(16, 11, 11)
+    inflow = np.zeros((3, 11, 11))
+    inflow[0, 1:-1, 1:-1] = 0.04
+    ball = lbm.ImmersedBoundary.from_ball(lbm.sphere(6.4, 5.3, 5.1, 1.7), spacing=1.0, iterations=3)
+
+    def make(scale):
+        s2, rules, d_rules = lbm.zou_he_inlet_derivative(lat, solid, scale * inflow)
+        return lbm.SimulationParams(nx=16, ny=11, nz=11, tau=0.6, collision="trt", solid=s2, dtype="float32",
+                                    link_rules=rules, immersed=ball), d_rules
+
+    p, _ = make(1.0)
+    run = AdjointRun(make, None, steps=12, window=4, checkpoint=4)
+    field = np.zeros((p.d, *p.shape))
+    run.forward(1.0, field)
+    out["ibm_adjoint_3d_backward_ms"] = timed(run.backward, 2) / 1e3
+    solid = lbm.duct_walls(256, 256, 256)
+    out["device_compiler_256_ms"] = timed(lambda: device_rules.ball_channel(lbm.D3Q19, lbm.sphere(256 / 3, 127.5, 127.5,
+                                                                                                 40.0), solid), 2) / 1e3
+    return out
+
+
 def max_over_ranks(x: float, world: int, device) -> float:
     """The largest value over all ranks (the slowest replica's time); x itself on one rank."""
     if world <= 1:
@@ -671,7 +758,7 @@ def run_ours(args, rank, world, local_rank):
     # ranks, the same on every rank. `ms_per_step` is the median repeat.
     with ClockSampler(uuid, interval_ms=50) as clocks:
         times = [timed_steps()]
-        repeats = int(min(MAX_REPEATS, max(MIN_REPEATS, math.ceil(MIN_TIMED_SECONDS * 1e3 / max(times[0], 1e-3)))))
+        repeats = int(min(MAX_REPEATS, max(MIN_REPEATS, math.ceil(args.repeat_seconds * 1e3 / max(times[0], 1e-3)))))
         for _ in range(repeats - 1):
             times.append(timed_steps())
     solver.time_step += warm + steps * len(times)
@@ -683,7 +770,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- the public run loop: the state check (NaN / rho <= 0 scan, float64 mass) fused into the
     # last step of every check_every-step chunk, read back with one small copy per chunk
     run_loop = None
-    if world == 1:
+    if world == 1 and args.run_loop:
         loop_steps, check_every = 2000, 500
         loop_steps += loop_steps % solver.step_multiple
         solver.run(check_every, check_every=check_every)  # warm: the checked-step kernel
@@ -792,7 +879,8 @@ def run_study(args):
     if args.study == "tgv":
         result = tgv_study(lbm, torch, **({"steps": k} if k else {}))
     elif args.study == "cylinder":
-        result = cylinder_study(lbm, torch, **({"steps": k} if k else {}))
+        methods = ("bouzidi", "ibm") if args.cylinder_method == "both" else (args.cylinder_method,)
+        result = cylinder_study(lbm, torch, methods=methods, **({"steps": k} if k else {}))
     elif args.study == "batched":
         result = batched_study(lbm, torch, **({"steps": k} if k else {}))
     elif args.study == "adjoint":
@@ -800,6 +888,8 @@ def run_study(args):
         result = adjoint_study(lbm, torch, **kw)
     elif args.study == "setup":
         result = setup_study(lbm, torch)
+    elif args.study == "kernels":
+        result = kernels_study(lbm, torch)
     else:
         result = precision_study(lbm, torch, args.n, k or args.precision_steps, args.variant)
     print(json.dumps({"study": args.study, "result": result}), flush=True)

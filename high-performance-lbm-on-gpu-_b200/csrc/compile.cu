@@ -123,10 +123,12 @@ __global__ void __launch_bounds__(COMPILE_THREADS) ball_links_count_kernel(const
     if (threadIdx.x < L::Q) offs[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = counts[threadIdx.x];
 }
 
-// Exclusive scan of offs[0 .. n) in place, total into offs[n]: one block of
-// 32 warps. Warp w scans the contiguous segment [w n/32, (w + 1) n/32) in
-// coalesced runs of 32 (a shuffle scan per run, carrying the running total);
-// the warp totals are then scanned in order and added back.
+// Exclusive scan of offs[0 .. n) in place, total into offs[n], in three
+// launches over blocks of SCAN_BLOCK entries: each block's sum into
+// sums[b]; one block scans those sums (exclusive, total into sums[nb]); each
+// block scans its entries and adds its offset.
+constexpr int SCAN_BLOCK = 1024;
+
 __device__ __forceinline__ int64_t warp_inclusive_scan(int64_t v, int lane)
 {
 #pragma unroll
@@ -137,35 +139,60 @@ __device__ __forceinline__ int64_t warp_inclusive_scan(int64_t v, int lane)
     return v;
 }
 
-__global__ void __launch_bounds__(1024) exclusive_scan_kernel(int64_t* __restrict__ offs, int64_t n)
+// Exclusive scan of one value per thread over a block of SCAN_BLOCK threads;
+// the block's total into *total.
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t* total)
 {
-    __shared__ int64_t warp_total[32];
+    __shared__ int64_t warp_sum[SCAN_BLOCK / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t seg = (n + 31) / 32;
-    const int64_t lo = warp * seg, hi = lo + seg < n ? lo + seg : n;
+    const int64_t inc = warp_inclusive_scan(v, lane);
+    if (lane == 31) warp_sum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int64_t w = warp_sum[lane];
+        const int64_t winc = warp_inclusive_scan(w, lane);
+        warp_sum[lane] = winc - w;
+        if (lane == 31) *total = winc;
+    }
+    __syncthreads();
+    return warp_sum[warp] + inc - v;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_sums_kernel(const int64_t* __restrict__ offs, int64_t n,
+                                                              int64_t* __restrict__ sums)
+{
+    __shared__ int64_t total;
+    const int64_t i = blockIdx.x * (int64_t)SCAN_BLOCK + threadIdx.x;
+    block_exclusive_scan(i < n ? offs[i] : 0, &total);
+    __syncthreads();
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// One block over nb (<= any size) block sums: runs of SCAN_BLOCK carried in order.
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_spine_kernel(int64_t* __restrict__ sums, int64_t nb)
+{
+    __shared__ int64_t total;
     int64_t carry = 0;
-    for (int64_t base = lo; base < hi; base += 32) {
-        const int64_t i = base + lane;
-        const int64_t v = i < hi ? offs[i] : 0;
-        const int64_t inc = warp_inclusive_scan(v, lane);
-        if (i < hi) offs[i] = carry + inc - v;
-        carry += __shfl_sync(0xffffffffu, inc, 31);
+    for (int64_t base = 0; base < nb; base += SCAN_BLOCK) {
+        const int64_t i = base + threadIdx.x;
+        const int64_t v = i < nb ? sums[i] : 0;
+        const int64_t ex = block_exclusive_scan(v, &total);
+        if (i < nb) sums[i] = carry + ex;
+        __syncthreads();
+        carry += total;
+        __syncthreads();
     }
-    if (lane == 0) warp_total[warp] = carry;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int64_t run = 0;
-        for (int w = 0; w < 32; ++w) {
-            const int64_t v = warp_total[w];
-            warp_total[w] = run;
-            run += v;
-        }
-        offs[n] = run;
-    }
-    __syncthreads();
-    const int64_t add = warp_total[warp];
-    if (add != 0)
-        for (int64_t i = lo + lane; i < hi; i += 32) offs[i] += add;
+    if (threadIdx.x == 0) sums[nb] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_apply_kernel(int64_t* __restrict__ offs, int64_t n,
+                                                               const int64_t* __restrict__ sums, int64_t nb)
+{
+    __shared__ int64_t total;
+    const int64_t i = blockIdx.x * (int64_t)SCAN_BLOCK + threadIdx.x;
+    const int64_t ex = block_exclusive_scan(i < n ? offs[i] : 0, &total);
+    if (i < n) offs[i] = sums[blockIdx.x] + ex;
+    if (blockIdx.x == 0 && threadIdx.x == 0) offs[n] = sums[nb];
 }
 
 // Pass 2: the links of direction j of this block go to offs[j * blocks + block]
@@ -303,9 +330,13 @@ int ball_links_count(const lbm_grid_t& g, BallArgs b, const uint8_t* solid, int6
 {
     const unsigned blocks = link_blocks(g);
     const int64_t n = (int64_t)L::Q * blocks;
+    const int64_t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    int64_t* sums = offs + n + 2;  // nb + 1 entries after the two result words
     if (cudaMemsetAsync(offs + n + 1, 0, sizeof(int64_t), s) != cudaSuccess) return LBM_ERR_LAUNCH;
     ball_links_count_kernel<L><<<blocks, COMPILE_THREADS, 0, s>>>(g, b, solid, offs);
-    exclusive_scan_kernel<<<1, 1024, 0, s>>>(offs, n);
+    scan_sums_kernel<<<(unsigned)nb, SCAN_BLOCK, 0, s>>>(offs, n, sums);
+    scan_spine_kernel<<<1, SCAN_BLOCK, 0, s>>>(sums, nb);
+    scan_apply_kernel<<<(unsigned)nb, SCAN_BLOCK, 0, s>>>(offs, n, sums, nb);
     return launch_status();
 }
 
@@ -356,7 +387,8 @@ static int lattice_q(int lattice) { return lattice == LBM_D2Q9 ? 9 : 19; }
 extern "C" int64_t lbm_ball_links_scratch(const lbm_grid_t* g)
 {
     if (!compile_grid_ok(g)) return LBM_ERR_INVALID;
-    return (int64_t)lattice_q(g->lattice) * link_blocks(*g) + 2;
+    const int64_t n = (int64_t)lattice_q(g->lattice) * link_blocks(*g);
+    return n + 2 + (n + SCAN_BLOCK - 1) / SCAN_BLOCK + 1;  // counts, two result words, the scan's block sums
 }
 
 extern "C" int lbm_ball_voxelize(const lbm_grid_t* g, double cx, double cy, double cz, double radius_sq, uint8_t* solid,

@@ -598,6 +598,70 @@ __global__ void __launch_bounds__(256) lbm_bulk_vec_aa_kernel(const StepArgs a)
     VecAA<L, ST, VAR>::run(a, warp_x * 64, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
 
+// ---------------------------------------------------------------- odd AA, rows
+// The odd AA half for float32/float64 with one block per row (nx <= 256):
+// a row whose nodes are all interior in y and z (kinds 0 and EDGE, the row off
+// the y and z faces) pulls and collides each node as the interior path does
+// (x wrapped in the row), writes its results into shared memory in
+// destination order -- f*_i of node x at x + c_x, wrapped -- and then stores
+// every direction's destination row (y + c_y, z + c_z) whole, each thread one
+// aligned element: the pushes along x no longer store to rows shifted by one
+// element, which half-fill 32-byte sectors that other warps complete. Other
+// rows run the one-node path (bulk_node). Same bits as the one-node kernel.
+// In place is safe: slot i of row (y + c_y, z + c_z) is read, in this half,
+// only by the nodes of row (y, z) -- this block -- before the block's barrier.
+template <class L, int ST, int CM>
+__global__ void __launch_bounds__(256) lbm_aa_odd_rows_kernel(const StepArgs a)
+{
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    constexpr int Q = L::Q;
+    extern __shared__ __align__(16) unsigned char rows_smem[];
+    T* out = reinterpret_cast<T*>(rows_smem);
+    advance_seed(a);
+    const int nx = a.nx, y = blockIdx.x, z = blockIdx.y, x = threadIdx.x;
+    const bool in = x < nx;
+    const int64_t py = a.pitch, pz = (int64_t)a.pitch * a.ny, qs = a.qstride;
+    const int64_t row = (int64_t)z * pz + (int64_t)y * py;
+    const int64_t nd = row + x;
+    const uint8_t k = in ? a.kind[nd] : KIND_FLUID;
+    const bool row_ok = y >= 1 && y <= a.ny - 2 && (L::D == 2 || (z >= 1 && z <= a.nz - 2));
+    if (!__syncthreads_and(row_ok && (k & ~KIND_EDGE) == 0)) {
+        bulk_node<L, ST, LBM_AA_ODD, false, CM>(a, x, y, z, nd, in);
+        return;
+    }
+    if (in) {
+        const int xm = x == 0 ? nx - 1 : x - 1, xp = x + 1 == nx ? 0 : x + 1;
+        const T* f = static_cast<const T*>(a.f_src);
+        R fv[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int sx = L::cx(i) > 0 ? xm : (L::cx(i) < 0 ? xp : x);
+            fv[i] = S::load(f + (L::opp(i) * qs + row - (L::cy(i) * py + L::cz(i) * pz) + sx));
+        }
+        R Fx = R(a.fx), Fy = R(a.fy), Fz = R(a.fz);
+        if (a.force_field != nullptr) {
+            const R* ff = static_cast<const R*>(a.force_field);
+            Fx += ff[nd];
+            Fy += ff[qs + nd];
+            if (L::D == 3) Fz += ff[2 * qs + nd];
+        }
+        collide_model<L, R, CM>(fv, a.template relax<R>(), a.guo_const && a.force_field == nullptr, Fx, Fy, Fz);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int dx = L::cx(i) > 0 ? xp : (L::cx(i) < 0 ? xm : x);
+            out[i * nx + dx] = S::encode(fv[i]);
+        }
+    }
+    __syncthreads();
+    if (in) {
+        T* f = static_cast<T*>(a.f_dst);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i * qs + row + (L::cy(i) * py + L::cz(i) * pz) + x] = out[i * nx + x];
+    }
+}
+
 // Storage formats with the pair and TMA kernels (float32 and float64 keep
 // the one-node kernel: it is faster there).
 template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_BF16; }
@@ -734,6 +798,14 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
             if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
                 const unsigned gxv = (unsigned)((a.nx + 2 * tile_x - 1) / (2 * tile_x));
                 lbm_bulk_vec_kernel<L, ST><<<dim3(gxv, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+                return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+            }
+        }
+        if constexpr (VAR == LBM_AA_ODD && !has_vec<ST>()) {
+            if (a.nx <= 256 && a.ny <= 65535) {
+                const unsigned threads = (unsigned)((a.nx + 31) / 32 * 32);
+                const size_t smem = (size_t)L::Q * a.nx * sizeof(typename Storage<ST>::T);
+                lbm_aa_odd_rows_kernel<L, ST, CM><<<dim3((unsigned)a.ny, (unsigned)a.nz), threads, smem, stream>>>(a);
                 return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
             }
         }

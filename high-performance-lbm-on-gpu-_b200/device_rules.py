@@ -93,7 +93,8 @@ def wall_links_device(lattice: VelocitySet, body, mask, shape):
     scratch = torch.empty(n_scratch, dtype=torch.int64, device="cuda")
     stream = _stream(torch)
     N.call("lbm_ball_links_count", N.C.byref(grid), N.ptr(mask), cx, cy, cz, r2, N.ptr(scratch), stream)
-    count, stray = (int(v) for v in scratch[-2:].cpu().tolist())
+    m = lattice.q * ((grid.qstride + 255) // 256)  # the per-(direction, block) counts come first
+    count, stray = (int(v) for v in scratch[m:m + 2].cpu().tolist())
     if stray:
         raise ValueError("every node inside the body must be marked solid")
     node = torch.empty(count, dtype=torch.int64, device="cuda")

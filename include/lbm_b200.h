@@ -318,9 +318,10 @@ int lbm_ball_voxelize(const lbm_grid_t* grid, double cx, double cy, double cz, d
  * wrap), ordered by direction j then node, with the wall fraction q along the
  * link (first root of |x - t c_j - centre| = R, clipped to (0, 1]) -- replaces
  * wall_links(lattice, body, solid) (src/lbm/geometry.py:174-206, 78-87).
- * Two passes over a scratch of lbm_ball_links_scratch(grid) int64:
- * lbm_ball_links_count leaves the link count in scratch[n - 2] and the number of
- * nodes inside the ball that are not solid (must be 0) in scratch[n - 1];
+ * Two passes over a scratch of lbm_ball_links_scratch(grid) int64 (with
+ * m = Q * ceil(qstride / 256) per-(direction, block) counts in front):
+ * lbm_ball_links_count leaves the link count in scratch[m] and the number of
+ * nodes inside the ball that are not solid (must be 0) in scratch[m + 1];
  * lbm_ball_links_write (same arguments and scratch) fills node[count],
  * direction[count], q[count]. */
 int64_t lbm_ball_links_scratch(const lbm_grid_t* grid);
