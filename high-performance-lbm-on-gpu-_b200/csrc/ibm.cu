@@ -26,8 +26,18 @@ __device__ __forceinline__ void ibm_moments_node(const lbm_grid_t& g, const lbm_
 {
     using R = typename Storage<ST>::R;
     const int64_t nd = ib.node[n];
-    const int64_t row = nd / g.pitch;
-    const int x = (int)(nd - row * g.pitch), y = (int)(row % g.ny), z = (int)(row / g.ny);
+    int x, y, z;
+    if (g.qstride <= 0x7fffffffLL) {  // 32-bit index arithmetic (a 64-bit division is a long subroutine)
+        const int row = (int)nd / g.pitch;
+        x = (int)nd - row * g.pitch;
+        y = row % g.ny;
+        z = row / g.ny;
+    } else {
+        const int64_t row = nd / g.pitch;
+        x = (int)(nd - row * g.pitch);
+        y = (int)(row % g.ny);
+        z = (int)(row / g.ny);
+    }
     R drho = R(0), jx = R(0), jy = R(0), jz = R(0);
 #pragma unroll
     for (int k = 0; k < L::Q; ++k) {
@@ -88,8 +98,11 @@ constexpr int IBM_FUSED_MAX = 4096;
 
 // MODE 1: bodies whose node and marker arrays fit in 48 KB keep a copy of
 // them in shared memory (rho, u*, the node force of the previous and the
-// current pass, the marker forces of the pass), so the phases read shared
-// memory instead of L2; the global arrays are written as well (the step,
+// current pass, the marker forces of the pass, and each node's velocity
+// correction F_n / (2 rho_n) of the previous pass -- formed once per node in
+// the node phase, where its divisions run in parallel over the nodes, instead
+// of 2 d divisions per stencil entry in every marker's chain: the same
+// operands, so the same bits), so the phases read shared memory instead of L2; the global arrays are written as well (the step,
 // the body force and the adjoint read them). MODE 2: when the body's tables
 // (stencils, weights, areas, the inverse CSR) fit beside them, they are
 // copied in too, all with independent loads in one phase, and the passes
@@ -97,7 +110,7 @@ constexpr int IBM_FUSED_MAX = 4096;
 template <class L, int ST>
 __host__ __device__ constexpr int64_t ibm_smem_reals(int nn, int nm)
 {
-    return (int64_t)nn * (1 + 3 * L::D) + (int64_t)L::D * nm;
+    return (int64_t)nn * (1 + 4 * L::D) + (int64_t)L::D * nm;
 }
 // The tables: real weight[nm S], area[nm], inv_weight[nm S], then int32
 // stencil[nm S], inv_start[nn + 1], inv_marker[nm S] (the inverse CSR lists
@@ -126,6 +139,7 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
     R* s_us = SMEM ? s_rho + nn : nullptr;
     R* s_f = SMEM ? s_us + D * nn : nullptr;  // two passes: [2][D][nn]
     R* s_mf = SMEM ? s_f + 2 * D * nn : nullptr;
+    R* s_corr = SMEM ? s_mf + D * nm : nullptr;  // [D][nn]: F_n / (2 rho_n) of the previous pass
     const int* stencil = ib.stencil;
     const R* wgt = (const R*)ib.weight;
     const R* area = (const R*)ib.area;
@@ -134,7 +148,7 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
     const R* invw = (const R*)ib.inv_weight;
     if constexpr (MODE == 2) {
         const int pairs = nm * S;
-        R* t_w = s_mf + D * nm;
+        R* t_w = s_corr + D * nn;
         R* t_area = t_w + pairs;
         R* t_invw = t_area + nm;
         int* t_st = reinterpret_cast<int*>(t_invw + pairs);
@@ -201,7 +215,7 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
 #pragma unroll
                 for (int a = 0; a < D; ++a) {
                     R u = us[a * nn + m[s]];
-                    if (fin != nullptr) u += fin[a * nn + m[s]] / (R(2) * rm);
+                    if (fin != nullptr) u += SMEM ? s_corr[a * nn + m[s]] : fin[a * nn + m[s]] / (R(2) * rm);
                     U[a] += w[s] * u;
                 }
             }
@@ -228,7 +242,10 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
                 const double base = fin != nullptr ? (double)fin[a * nn + n] : 0.0;
                 const R v = (R)(base + acc[a]);
                 fout[a * nn + n] = v;
-                if (SMEM) s_fout[a * nn + n] = v;
+                if (SMEM) {
+                    s_fout[a * nn + n] = v;
+                    s_corr[a * nn + n] = v / (R(2) * rho[n]);  // read by the next pass's markers
+                }
             }
         }
         __syncthreads();

@@ -78,6 +78,10 @@ class SimulationParams:
     immersed: object | None = field(default=None, kw_only=True, repr=False)
 
     def __post_init__(self) -> None:
+        """Validate and freeze. The checks, their order and their error messages are the
+        reference's (``params.py:129-175``) statement for statement, on purpose: they are the
+        drop-in's input contract, pinned by ``tests/test_builders_golden.py``. The additions are
+        the 16-bit storage formats and the ``"regularized"`` collision model."""
         sizes = {"nx": self.nx, "ny": self.ny} | ({} if self.nz is None else {"nz": self.nz})
         if any(n <= 0 for n in sizes.values()):
             got = ", ".join(f"{k}={v}" for k, v in sizes.items())
