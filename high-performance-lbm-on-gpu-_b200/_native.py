@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -131,6 +131,7 @@ _SIGNATURES = {
     "lbm_ibm_moments": [P(Grid), P(Physics), P(Ibm), vp, i32, vp],
     "lbm_ibm_iteration": [P(Grid), P(Ibm), i32, vp, vp, vp],
     "lbm_ibm_force": [P(Grid), P(Physics), P(Ibm), vp, i32, i32, vp, vp],
+    "lbm_step_pull_ibm": [P(Grid), P(Physics), P(Special), P(Ibm), i32, vp, vp, vp, vp, vp],
     "lbm_ibm_body_force": [P(Grid), P(Ibm), i32, vp, vp],
     "lbm_ibm_adjoint_iteration": [P(Grid), P(Ibm), vp, vp, i32, C.c_double, vp, vp, vp],
     "lbm_ibm_adjoint_moments": [P(Grid), P(Ibm), vp, vp, vp],

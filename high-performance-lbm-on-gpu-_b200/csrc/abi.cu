@@ -11,7 +11,9 @@ static int record(int status)
     return status;
 }
 
-static bool grid_valid(const lbm_grid_t* g)
+namespace lbm {
+
+bool grid_valid(const lbm_grid_t* g)
 {
     if (g == nullptr) return false;
     if (g->lattice != LBM_D2Q9 && g->lattice != LBM_D3Q19) return false;
@@ -21,7 +23,7 @@ static bool grid_valid(const lbm_grid_t* g)
     return g->qstride >= (int64_t)g->pitch * g->ny * g->nz;
 }
 
-static bool special_valid(const lbm_special_t* sp, bool aa)
+bool special_valid(const lbm_special_t* sp, bool aa)
 {
     if (sp == nullptr) return true;
     if (sp->n_special < 0 || sp->n_rules < 0 || sp->n_terms < 0 || sp->n_local < 0 || sp->n_export < 0) return false;
@@ -55,7 +57,7 @@ static int64_t health_partials(const lbm_grid_t* g, const lbm_special_t* sp, int
     return gx * gy * g->nz + (ns + BOUNDARY_THREADS - 1) / BOUNDARY_THREADS;
 }
 
-static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
+int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
                      const lbm_launch_t* launch, const uint8_t* kind, const void* src, void* dst, int& tx, int& ty,
                      int& mode)
 {
@@ -113,6 +115,8 @@ static int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, c
     }
     return LBM_OK;
 }
+
+}  // namespace lbm
 
 template <class L, int ST>
 static int step_dispatch(const StepArgs& a, int variant, int mode, int tx, int ty, cudaStream_t s)
@@ -176,4 +180,4 @@ extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t wh
 
 extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
 
-extern "C" int32_t lbm_abi_version(void) { return 7; }
+extern "C" int32_t lbm_abi_version(void) { return 8; }

@@ -8,6 +8,12 @@ namespace lbm {
 template <class L, int ST> int launch_step(const StepArgs& a, int variant, int mode, int tile_x, int tile_y, cudaStream_t stream);
 template <class L, int ST> int step_resources(int variant, int32_t* out4);
 
+// Argument checks and StepArgs of the step entry points (abi.cu); launch may be null (defaults).
+bool grid_valid(const lbm_grid_t* g);
+bool special_valid(const lbm_special_t* sp, bool aa);
+int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
+              const lbm_launch_t* launch, const uint8_t* kind, const void* src, void* dst, int& tx, int& ty, int& mode);
+
 // Invoke FN<L, ST>(args...) for the run-time lattice and storage codes.
 #define LBM_DISPATCH(lattice, storage, FN, ...)                                            \
     do {                                                                                   \

@@ -15,6 +15,7 @@
 //             for the body force. Markers are recomputed by each of their
 //             3^d nodes, which is cheaper than a second launch per pass.
 #include "dispatch.cuh"
+#include "step_kernels.cuh"
 
 namespace lbm {
 
@@ -22,10 +23,10 @@ template <class L, int ST>
 __device__ __forceinline__ void ibm_moments_node(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib,
                                                  const typename Storage<ST>::T* __restrict__ f, int layout, int n,
                                                  typename Storage<ST>::R* s_rho = nullptr,
-                                                 typename Storage<ST>::R* s_us = nullptr)
+                                                 typename Storage<ST>::R* s_us = nullptr, int64_t nd_loaded = -1)
 {
     using R = typename Storage<ST>::R;
-    const int64_t nd = ib.node[n];
+    const int64_t nd = nd_loaded >= 0 ? nd_loaded : ib.node[n];
     int x, y, z;
     if (g.qstride <= 0x7fffffffLL) {  // 32-bit index arithmetic (a 64-bit division is a long subroutine)
         const int row = (int)nd / g.pitch;
@@ -125,9 +126,9 @@ __host__ __device__ constexpr int64_t ibm_table_bytes(int nn, int nm)
 constexpr int64_t IBM_SMEM_BYTES = 48 * 1024;
 
 template <class L, int ST, int MODE>
-__global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel(
-    const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib, const typename Storage<ST>::T* __restrict__ f,
-    int layout, int iterations, typename Storage<ST>::R* force)
+__device__ __forceinline__ void ibm_force_block(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib,
+                                                const typename Storage<ST>::T* __restrict__ f, int layout,
+                                                int iterations, typename Storage<ST>::R* force)
 {
     using R = typename Storage<ST>::R;
     constexpr int D = L::D;
@@ -146,6 +147,8 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
     const int* inv_start = ib.inv_start;
     const int* inv_marker = ib.inv_marker;
     const R* invw = (const R*)ib.inv_weight;
+    // the thread's first stencil node, loaded ahead of the tables (the moments need it): one round trip fewer
+    const int64_t nd0 = (int)threadIdx.x < nn ? ib.node[threadIdx.x] : 0;
     if constexpr (MODE == 2) {
         const int pairs = nm * S;
         R* t_w = s_corr + D * nn;
@@ -155,26 +158,36 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
         int* t_is = t_st + pairs;
         int* t_im = t_is + nn + 1;
         const int count = pairs > nn + 1 ? pairs : nn + 1;
-        for (int i = threadIdx.x; i < count; i += blockDim.x) {
-            // every load of the entry first, then the stores: one round trip
-            int st = 0, im = 0, is = 0;
-            R w = R(0), iw = R(0), ar = R(0);
-            if (i < pairs) {
-                st = ib.stencil[i];
-                w = wgt[i];
-                im = ib.inv_marker[i];
-                iw = invw[i];
+        constexpr int U = 4;  // entries per thread per round trip: every load of them first, then the stores
+        for (int i0 = threadIdx.x; i0 < count; i0 += U * blockDim.x) {
+            int st[U], im[U], is[U];
+            R w[U], iw[U], ar[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * blockDim.x;
+                st[u] = im[u] = is[u] = 0;
+                w[u] = iw[u] = ar[u] = R(0);
+                if (i < pairs) {
+                    st[u] = ib.stencil[i];
+                    w[u] = wgt[i];
+                    im[u] = ib.inv_marker[i];
+                    iw[u] = invw[i];
+                }
+                if (i <= nn) is[u] = ib.inv_start[i];
+                if (i < nm) ar[u] = area[i];
             }
-            if (i <= nn) is = ib.inv_start[i];
-            if (i < nm) ar = area[i];
-            if (i < pairs) {
-                t_st[i] = st;
-                t_w[i] = w;
-                t_im[i] = im;
-                t_invw[i] = iw;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < pairs) {
+                    t_st[i] = st[u];
+                    t_w[i] = w[u];
+                    t_im[i] = im[u];
+                    t_invw[i] = iw[u];
+                }
+                if (i <= nn) t_is[i] = is[u];
+                if (i < nm) t_area[i] = ar[u];
             }
-            if (i <= nn) t_is[i] = is;
-            if (i < nm) t_area[i] = ar;
         }
         stencil = t_st;
         wgt = t_w;
@@ -183,7 +196,8 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
         inv_marker = t_im;
         invw = t_invw;
     }
-    for (int n = threadIdx.x; n < nn; n += blockDim.x) ibm_moments_node<L, ST>(g, p, ib, f, layout, n, s_rho, s_us);
+    for (int n = threadIdx.x; n < nn; n += blockDim.x)
+        ibm_moments_node<L, ST>(g, p, ib, f, layout, n, s_rho, s_us, n == (int)threadIdx.x ? nd0 : -1);
     __syncthreads();
     const R* rho = SMEM ? s_rho : (const R*)ib.rho;
     const R* us = SMEM ? s_us : (const R*)ib.u_star;
@@ -250,6 +264,36 @@ __global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel
         }
         __syncthreads();
     }
+}
+
+template <class L, int ST, int MODE>
+__global__ void __launch_bounds__(ibm_fused_threads<L>()) ibm_force_fused_kernel(
+    const lbm_grid_t g, const lbm_physics_t p, const lbm_ibm_t ib, const typename Storage<ST>::T* __restrict__ f,
+    int layout, int iterations, typename Storage<ST>::R* force)
+{
+    ibm_force_block<L, ST, MODE>(g, p, ib, f, layout, iterations, force);
+}
+
+// The immersed-boundary part of a pull step in one block: the body force of
+// the step (as ibm_force_fused_kernel), then the update of the special nodes
+// of a.sp -- the body's stencil nodes -- with the final pass's node force,
+// by the boundary warps' node path (boundary_node: same operations, same
+// bits). The last pass ends with a block barrier, after which the node force
+// written to global memory is visible to every thread of the block. The step's
+// other special nodes and its bulk run in concurrent launches, so no launch of
+// the step waits for the force. 512 threads in 2D too: the node update needs
+// more than the 64 registers a thread of a 1024-thread block can have.
+template <class L> constexpr int ibm_step_threads() { return 512; }
+
+template <class L, int ST, int MODE, int CM>
+__global__ void __launch_bounds__(ibm_step_threads<L>()) ibm_step_kernel(const StepArgs a, const lbm_grid_t g,
+                                                                          const lbm_physics_t p, const lbm_ibm_t ib,
+                                                                          int iterations,
+                                                                          typename Storage<ST>::R* force)
+{
+    ibm_force_block<L, ST, MODE>(g, p, ib, static_cast<const typename Storage<ST>::T*>(a.f_src), LBM_LAYOUT_PULL,
+                                 iterations, force);
+    for (int64_t s = threadIdx.x; s < a.sp.n_special; s += blockDim.x) boundary_node<L, ST, LBM_PULL, false, CM>(a, s);
 }
 
 template <class L, int ST>
@@ -679,6 +723,37 @@ int ibm_force(const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, 
     return launch_status();
 }
 
+template <class L, int ST, int CM>
+int ibm_step_model(StepArgs a, const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, int iterations,
+                   void* force, cudaStream_t s)
+{
+    using R = typename Storage<ST>::R;
+    R* out = (R*)force;
+    a.sp.local_force = out + (int64_t)(iterations - 1) * L::D * ib.n_nodes;  // the final pass
+    a.sp.n_local = ib.n_nodes;
+    constexpr int threads = ibm_step_threads<L>();
+    const int64_t smem = ibm_smem_reals<L, ST>(ib.n_nodes, ib.n_markers) * (int64_t)sizeof(R);
+    const int64_t with_tables = smem + ibm_table_bytes<L, ST>(ib.n_nodes, ib.n_markers);
+    if (with_tables <= IBM_SMEM_BYTES)
+        ibm_step_kernel<L, ST, 2, CM><<<1, threads, (size_t)with_tables, s>>>(a, g, p, ib, iterations, out);
+    else if (smem <= IBM_SMEM_BYTES)
+        ibm_step_kernel<L, ST, 1, CM><<<1, threads, (size_t)smem, s>>>(a, g, p, ib, iterations, out);
+    else if (ib.n_nodes <= IBM_FUSED_MAX && ib.n_markers <= IBM_FUSED_MAX)
+        ibm_step_kernel<L, ST, 0, CM><<<1, threads, 0, s>>>(a, g, p, ib, iterations, out);
+    else
+        return LBM_ERR_UNSUPPORTED;
+    return launch_status();
+}
+
+template <class L, int ST>
+int ibm_step(const StepArgs& a, const lbm_grid_t& g, const lbm_physics_t& p, const lbm_ibm_t& ib, int iterations,
+             void* force, cudaStream_t s)
+{
+    if (a.collision == LBM_COLLIDE_REGULARIZED)
+        return ibm_step_model<L, ST, LBM_COLLIDE_REGULARIZED>(a, g, p, ib, iterations, force, s);
+    return ibm_step_model<L, ST, LBM_COLLIDE_TRT>(a, g, p, ib, iterations, force, s);
+}
+
 template <class L, int ST>
 int ibm_iteration(const lbm_grid_t& g, const lbm_ibm_t& ib, int iteration, const void* fin, void* fout, cudaStream_t s)
 {
@@ -726,6 +801,22 @@ extern "C" int lbm_ibm_force(const lbm_grid_t* g, const lbm_physics_t* p, const 
     if (!ibm_ok(g, ib) || !p || !f || !force || iterations < 1) return LBM_ERR_INVALID;
     if (layout < LBM_LAYOUT_PULL || layout > LBM_LAYOUT_AA_EVEN) return LBM_ERR_INVALID;
     LBM_DISPATCH(g->lattice, g->storage, ibm_force, *g, *p, *ib, f, layout, iterations, force, (cudaStream_t)stream);
+}
+
+extern "C" int lbm_step_pull_ibm(const lbm_grid_t* g, const lbm_physics_t* p, const lbm_special_t* sp,
+                                 const lbm_ibm_t* ib, int32_t iterations, const uint8_t* kind, const void* f_src,
+                                 void* f_dst, void* force, lbm_stream_t stream)
+{
+    if (!grid_valid(g) || !ibm_ok(g, ib) || !p || !sp || !kind || !f_src || !f_dst || f_src == f_dst || !force ||
+        iterations < 1 || !special_valid(sp, false))
+        return LBM_ERR_INVALID;
+    if (ib->n_nodes <= 0 || (sp->n_special > 0 && !sp->force_slot)) return LBM_ERR_INVALID;
+    StepArgs a;
+    int tx = 0, ty = 0, mode = 0;
+    const int st = make_args(a, g, p, sp, nullptr, kind, f_src, f_dst, tx, ty, mode);
+    if (st != LBM_OK) return st;
+    a.parity = (uintptr_t)f_src > (uintptr_t)f_dst ? 1 : 0;
+    LBM_DISPATCH(g->lattice, g->storage, ibm_step, a, *g, *p, *ib, iterations, force, (cudaStream_t)stream);
 }
 
 extern "C" int lbm_ibm_iteration(const lbm_grid_t* g, const lbm_ibm_t* ib, int32_t iteration, const void* force_in,

@@ -305,6 +305,7 @@ class CudaSolver(Solver):
             self._ibm = _IbmState(self, build_tables(params.immersed, lattice, np.asarray(params.solid)))
         self._solid_host = np.asarray(params.solid, dtype=bool)
         self._special = self._build_special(params)
+        self._ibm_split = self._split_special()
 
         # ---- populations
         self._f = torch.empty((q, self.qstride), dtype=self.t_store, device=self.device)
@@ -466,6 +467,36 @@ class CudaSolver(Solver):
         t["export_first"] = torch.from_numpy(export_first).to(self.device)
         return _SpecialTables(t, ns, n_rules, n_terms, n_export, int(ibm_nodes.size))
 
+    def _split_special(self):
+        """The boundary-warp list of a pull step with an immersed body, cut in two: the body's
+        stencil nodes, which ``lbm_step_pull_ibm`` updates in the launch that forms their force, and
+        the rest, for a boundary launch beside it. None (one list, force then boundary launch) for
+        the AA variant, a body beyond the one-block kernel, or a stencil node that also has rules."""
+        sp, ibm = self._special, self._ibm
+        if ibm is None or self.variant != "pull" or sp.n_special == 0:
+            return None
+        if ibm.tables.n_nodes > N.IBM_FUSED_MAX or ibm.tables.n_markers > N.IBM_FUSED_MAX:
+            return None
+        t = sp.tensors
+        on_body = (t["force_slot"] >= 0).cpu().numpy()
+        if np.any(t["rule_mask"].cpu().numpy()[on_body] != 0):
+            return None
+        torch, dev = self.torch, self.device
+        rest = torch.from_numpy(np.flatnonzero(~on_body)).to(dev)
+        body = torch.from_numpy(np.flatnonzero(on_body)).to(dev)
+        per_node = ("node", "rule_mask", "rule_first", "force_slot", "export_mask", "export_first")
+        shared = {k: v for k, v in t.items() if k not in per_node and k != "ut_start"}
+        t_rest = {k: t[k][rest] for k in per_node} | shared
+        if "ut_start" in t:
+            # stencil nodes have no rules, so their distinct-term ranges are empty: the other
+            # nodes' ranges stay contiguous
+            t_rest["ut_start"] = torch.cat([t["ut_start"][rest], t["ut_start"][-1:]])
+        t_body = {k: t[k][body] for k in ("node", "force_slot")}
+        t_body["rule_mask"] = torch.zeros_like(t_body["force_slot"])
+        t_body["rule_first"] = torch.zeros_like(t_body["force_slot"])
+        return (_SpecialTables(t_rest, int(rest.numel()), sp.n_rules, sp.n_terms, sp.n_export, 0),
+                _SpecialTables(t_body, int(body.numel()), 0, 0, 0, sp.n_local))
+
     def _dense_rules(self, t, nodes, rule_nodes, start, term_slot, term_coeff) -> None:
         """Dense form of the rules on the device (``dense_rule_tables``); left out (term-by-term
         evaluation) when a node's rules read more than ``DENSE_TERMS`` distinct populations."""
@@ -497,8 +528,8 @@ class CudaSolver(Solver):
         self._checked_launches = {m: N.Launch(bx, by, m, 0, N.C.pointer(self._health_struct))
                                   for m in N.LAUNCH_MODES}
 
-    def _special_struct(self, export_in=None, export_out=None) -> N.Special:
-        s = self._special
+    def _special_struct(self, export_in=None, export_out=None, tables=None) -> N.Special:
+        s = self._special if tables is None else tables
         t = s.tensors
         g = t.get
         local = self._ibm.final_force if self._ibm is not None else None
@@ -690,7 +721,48 @@ class CudaSolver(Solver):
             s = self._side = self.torch.cuda.Stream(self.device)
         return s
 
+    def _step_pull_ibm(self) -> None:
+        """A pull step with an immersed body, three launches on three streams, none waiting on
+        another: the body force and its stencil nodes' update (``lbm_step_pull_ibm``), the other
+        special nodes (boundary launch), the bulk."""
+        torch = self.torch
+        g, ph = N.C.byref(self.grid), N.C.byref(self.physics)
+        rest, body = self._ibm_split
+        ibm = self._ibm
+        main = torch.cuda.current_stream(self.device)
+        sides = self._side_streams(2)
+        fork = torch.cuda.Event()
+        fork.record(main)
+        joins = []
+        for side in sides:
+            side.wait_event(fork)
+        self._native("lbm_step_pull_ibm", g, ph, N.C.byref(self._special_struct(tables=body)), N.C.byref(ibm.struct),
+                     ibm.tables.iterations, N.ptr(self._kind), N.ptr(self._f), N.ptr(self._f_next), N.ptr(ibm.force),
+                     sides[0].cuda_stream)
+        if rest.n_special:
+            self._native("lbm_step_pull", g, ph, N.C.byref(self._special_struct(tables=rest)),
+                         N.C.byref(self._launches[N.LAUNCH_BOUNDARY]), N.ptr(self._kind), N.ptr(self._f),
+                         N.ptr(self._f_next), sides[1].cuda_stream)
+        for side in sides:
+            joins.append(torch.cuda.Event())
+            joins[-1].record(side)
+        self._native("lbm_step_pull", g, ph, N.C.byref(self._special_struct(tables=rest)),
+                     N.C.byref(self._launches[N.LAUNCH_BULK]), N.ptr(self._kind), N.ptr(self._f), N.ptr(self._f_next),
+                     main.cuda_stream)
+        for join in joins:
+            main.wait_event(join)
+        self._f, self._f_next = self._f_next, self._f
+
+    def _side_streams(self, n: int):
+        streams = getattr(self, "_sides", None)
+        if streams is None or len(streams) < n:
+            streams = self._sides = [self._side_stream] + [self.torch.cuda.Stream(self.device) for _ in range(n - 1)]
+        return streams[:n]
+
     def _launch_pull(self, checked=False):
+        if self._ibm_split is not None and not checked and self.launch_mode != "fused":
+            self._step_pull_ibm()
+            return
         # the immersed-boundary force reads f_src only and feeds only the boundary kernel
         f = self._f
         ibm = None if self._ibm is None else (lambda stream: self._ibm.run(f, N.LAYOUT_PULL, stream))

@@ -396,6 +396,22 @@ int lbm_ibm_iteration(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iter
 int lbm_ibm_force(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm_ibm_t* ibm, const void* f,
                   int32_t layout, int32_t iterations, void* force, lbm_stream_t stream);
 
+/* The immersed-boundary part of one pull step in one launch: lbm_ibm_force of
+ * f_src (layout LBM_LAYOUT_PULL, into force as there), then, in the same
+ * block, the step of the special nodes in sp -- the body's stencil nodes --
+ * from f_src into f_dst with the final pass's node force (sp->local_force and
+ * sp->n_local are set to it; force_slot indexes it), exactly as a
+ * LBM_LAUNCH_BOUNDARY launch of lbm_step_pull would update them. With the
+ * step's other special nodes in a BOUNDARY launch and the bulk in a BULK
+ * launch, all three concurrent, no launch of the step waits for the force
+ * (replaces lbm_ibm_force followed by a BOUNDARY launch over every special
+ * node; reference src/lbm/solver.py runs the force before each step,
+ * src/lbm/ibm.py:189-214). Bodies of up to 4096 stencil nodes and markers;
+ * larger ones return LBM_ERR_UNSUPPORTED. */
+int lbm_step_pull_ibm(const lbm_grid_t* grid, const lbm_physics_t* phys, const lbm_special_t* sp,
+                      const lbm_ibm_t* ibm, int32_t iterations, const uint8_t* kind, const void* f_src,
+                      void* f_dst, void* force, lbm_stream_t stream);
+
 /* Body force -sum_iterations sum_l F_l in float64 (out[d]). */
 int lbm_ibm_body_force(const lbm_grid_t* grid, const lbm_ibm_t* ibm, int32_t iterations, double* out,
                        lbm_stream_t stream);

@@ -111,7 +111,8 @@ def open_channel_case(ns, d=2, rho_out=1.003, dtype="float64"):
     return params, inflow
 
 
-def cylinder_channel(ns, method="bouzidi", nx=880, ny=164, dtype="float32", u_max=0.05, iterations=3):
+def cylinder_channel(ns, method="bouzidi", nx=880, ny=164, dtype="float32", u_max=0.05, iterations=3,
+                     center=(200.0, 82.0), radius=20.0):
     """Config: D2Q9 channel 880 x 164, cylinder D = 40 at (200, 82), Zou-He in/out, Re = 100.
 
     Parabolic inflow as the reference's Schaefer-Turek builder
@@ -125,7 +126,7 @@ def cylinder_channel(ns, method="bouzidi", nx=880, ny=164, dtype="float32", u_ma
     inflow = np.stack([profile, np.zeros(ny)])
     solid = np.zeros((ny, nx), dtype=bool)
     solid[0, :] = solid[-1, :] = True
-    body = ns.circle(200.0, 82.0, 20.0)
+    body = ns.circle(*center, radius)
     immersed = None
     if method == "ibm":
         immersed = ns.ImmersedBoundary.from_ball(body, spacing=1.0, iterations=iterations)

@@ -425,6 +425,40 @@ def test_fused_and_split_launches_give_identical_bits(backend, d):
     np.testing.assert_array_equal(a.populations(), b.populations())
 
 
+@pytest.mark.parametrize("case,dtype,collision", [
+    ("ibm2", "float64", "trt"), ("ibm2", "float32", "trt"), ("ibm2", "float16", "trt"), ("ibm3", "float32", "trt"),
+    ("ibm3", "bfloat16", "trt"), ("ibm2", "float32", "regularized"), ("cylinder", "float32", "trt"),
+    ("cylinder", "float64", "trt")])
+def test_immersed_body_step_in_one_launch_gives_the_boundary_launchs_bits(case, dtype, collision):
+    """A pull step with an immersed body updates the body's stencil nodes in the launch that
+    forms their force (lbm_step_pull_ibm), beside a boundary launch over the other special nodes
+    (the cylinder's Zou-He inlet and outlet, in the dense rule form) and the bulk; the fused
+    launch mode keeps the force followed by one boundary list. Same bits, over steps that feed
+    each step's force back into the populations (16-bit storage: same stochastic rounding)."""
+    import dataclasses
+
+    if case == "cylinder":
+        p = cases.cylinder_channel(NS, "ibm", nx=160, ny=60, dtype=dtype, center=(50.0, 30.0), radius=8.0)[0]
+        state = cases.random_state(p, seed=3, u_scale=0.03)
+    else:
+        p = cases.ibm(NS, 2 if case == "ibm2" else 3, dtype)
+        state = cases.random_state(p)
+    p = dataclasses.replace(p, collision=collision)
+    split = lbm.make_solver(p, backend="cuda-naive")
+    fused = lbm.make_solver(p, backend="cuda-naive", launch="fused")
+    assert split._ibm_split is not None and fused._ibm_split is not None
+    rest, body = split._ibm_split
+    assert body.n_special == split._ibm.tables.n_nodes
+    assert rest.n_special == split._special.n_special - body.n_special
+    if case == "cylinder":
+        assert rest.n_special > 0 and "ut_start" in rest.tensors
+    for s in (split, fused):
+        s.initialize(*state)
+        s.run(14)
+    np.testing.assert_array_equal(split.populations(), fused.populations())
+    np.testing.assert_array_equal(split.immersed_force, fused.immersed_force)
+
+
 @pytest.mark.parametrize("backend", BACKENDS)
 @pytest.mark.parametrize("block", [(32, 4), (64, 4), (128, 2), (32, 8), (256, 1)])
 def test_block_shapes_give_identical_bits(backend, block):
