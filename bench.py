@@ -572,7 +572,8 @@ def batched_study(lbm, torch, steps: int = 640, separate_steps: int = 20):
 def setup_study(lbm, torch):
     """Set-up time of two bodies in a channel, host builders against the device-side compiler
     (voxelisation, wall links, Bouzidi rules; the solver's own tables after): the sphere channel
-    (128 x 64 x 64, r = 8) and a 256^3 duct with a sphere of radius 40. Wall-clock seconds."""
+    (128 x 64 x 64, r = 8) and a 256^3 duct with a sphere of radius 40; then the Zou-He inlet and
+    outlet rules of open channels of both sizes. Wall-clock seconds."""
     from lbm_b200 import device_rules
 
     out = {}
@@ -605,6 +606,26 @@ def setup_study(lbm, torch):
                       "solver_tables_s": round(t_solver, 3)}
         del solver
         torch.cuda.empty_cache()
+    # Zou-He inlet and outlet rules of an open channel (walls y/z), host builder against the device
+    for label, n_x, n_yz in (("open_channel_128x64x64", 128, 64), ("open_channel_256x256x256", 256, 256)):
+        solid = lbm.duct_walls(n_x, n_yz, n_yz)
+        inflow = np.zeros((3, n_yz, n_yz))
+        inflow[0, 1:-1, 1:-1] = 0.04
+        device_rules.open_channel(lbm.D3Q19, solid, inflow)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ds, dr = device_rules.open_channel(lbm.D3Q19, solid, inflow)
+        t_dev = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hs, hr = lbm.open_channel(lbm.D3Q19, solid, inflow)
+        t_host = time.perf_counter() - t0
+        same = bool(np.array_equal(ds, hs) and all(
+            np.array_equal(a, b) for a, b in ((dr.node, hr.node), (dr.direction, hr.direction),
+                                              (dr.values.coeff, hr.values.coeff),
+                                              (dr.values.constant, hr.values.constant),
+                                              (dr.values.node, hr.values.node))))
+        out[label] = {"rules": len(hr), "host_builder_s": round(t_host, 4), "device_builder_s": round(t_dev, 4),
+                      "speedup": round(t_host / t_dev, 1), "identical": same}
     return out
 
 

@@ -141,8 +141,11 @@ _SIGNATURES = {
     "lbm_ball_links_write": [P(Grid), vp, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp, vp, vp, vp],
     "lbm_bouzidi_links": [P(Grid), vp, i64, vp, vp, vp, vp, vp, vp, vp, vp],
     "lbm_compile_terms": [P(Grid), i32, vp, vp, i64, vp, vp, vp, vp, vp, vp],
+    "lbm_zou_he_count": [P(Grid), vp, i32, i32, i32, vp, vp, C.c_double, vp, vp],
+    "lbm_zou_he_write": [P(Grid), vp, i32, i32, i32, vp, vp, C.c_double, vp, i32, vp, vp, vp, vp, vp, vp, vp],
 }
-EXPORTED = (*_SIGNATURES, "lbm_health_partials", "lbm_ball_links_scratch", "lbm_last_cuda_error", "lbm_abi_version")
+EXPORTED = (*_SIGNATURES, "lbm_health_partials", "lbm_ball_links_scratch", "lbm_zou_he_scratch",
+            "lbm_last_cuda_error", "lbm_abi_version")
 
 _lib = None
 
@@ -167,6 +170,8 @@ def load(path: Path | None = None):
     lib.lbm_health_partials.restype = i64
     lib.lbm_ball_links_scratch.argtypes = [P(Grid)]
     lib.lbm_ball_links_scratch.restype = i64
+    lib.lbm_zou_he_scratch.argtypes = [P(Grid)]
+    lib.lbm_zou_he_scratch.restype = i64
     lib.lbm_last_cuda_error.restype = C.c_char_p
     lib.lbm_last_cuda_error.argtypes = []
     lib.lbm_abi_version.restype = i32

@@ -9,6 +9,8 @@
 //   lbm_bouzidi_links      the Bouzidi rule of every link (reference link_rules.py:154-188)
 //   lbm_compile_terms      slots of affine terms in a stored layout (reference
 //                          link_rules.py:203-240), pitched for this library's buffers
+//   lbm_zou_he_count       \  the Zou-He rules of an open inlet or outlet column
+//   lbm_zou_he_write       /  (reference open_boundaries.py:96-186)
 //
 // Node positions are the integer coordinates (x, y[, z]); every floating-point
 // operation is an explicitly rounded IEEE operation in the order the host
@@ -316,6 +318,237 @@ __global__ void compile_terms_kernel(const lbm_grid_t g, int layout, const uint8
     if (extra != nullptr) extra[t] = e;
 }
 
+// ---------------------------------------------------------------- Zou-He rules
+// The rules of one open column x = column of a channel whose x = 0 and
+// x = nx - 1 layers are closed (reference open_boundaries.py:96-153, in the
+// Hecht-Harting form): velocity inlet (sign +1, velocity given at the
+// column) or density outlet (sign -1, rho_out). Node (x, y, z) of the column,
+// cross-section index c = z * ny + y, gets one rule per unknown population j
+// (sign * c_jx = +1, ascending j) when it is fluid and some unknown streams in
+// from the open layer (x - c_j in the layer, periodic wrap). A rule is a
+// coefficient row over the node's Q streamed populations s_k = f*_k(x - c_k),
+// or f*_opp(k)(x) when x - c_k is solid; with S0 + 2 S- = sum_k known_k s_k
+// (known_k = 1 for c_n = 0, 2 for c_n = -1):
+//   f_j = s_opp(j) + 6 w_j (c_j . rho u) - sum_t c_jt N_t,
+//   N_t = 1/2 sum_{c_n = 0} s_k c_kt - rho u_t / 3,
+//   inlet: rho u_a = u_a (S0 + 2 S-) / (1 - sign u_x); outlet: rho u_x = sign rho_out - sign (S0 + 2 S-),
+// plus the shifted-storage constant b - w_j + sum_k a_k w_k. Every value is
+// formed in the host builder's order, each operation rounded once.
+struct ZouHeArgs {
+    int column, sign;
+    int layer_x;             // x of the open layer
+    const uint8_t* layer;    // (nz * ny) fluid nodes of the open layer, before it was closed
+    const double* velocity;  // (d, nz * ny) prescribed velocity at the column; NULL: outlet at rho_out
+    double rho_out;
+};
+
+template <class L>
+__device__ __forceinline__ int lat_c(int k, int a)
+{
+    return a == 0 ? L::cx(k) : (a == 1 ? L::cy(k) : L::cz(k));
+}
+
+template <class L>
+__device__ __forceinline__ double zh_known(int k, int sign)
+{
+    const int cn = sign * L::cx(k);
+    return cn == 0 ? 1.0 : (cn == -1 ? 2.0 : 0.0);
+}
+
+// rho u_a as an affine form: coefficient of s_k, and constant.
+template <class L>
+__device__ __forceinline__ double zh_rho_u_coeff(const ZouHeArgs& z, const double* u, double denom, int a, int k)
+{
+    const double known = zh_known<L>(k, z.sign);
+    if (z.velocity != nullptr) return __dmul_rn(__ddiv_rn(known, denom), u[a]);
+    return a == 0 ? __dmul_rn((double)(-z.sign), known) : 0.0;
+}
+__device__ __forceinline__ double zh_rho_u_const(const ZouHeArgs& z, int a)
+{
+    return (z.velocity == nullptr && a == 0) ? __dmul_rn((double)z.sign, z.rho_out) : 0.0;
+}
+
+template <class L>
+__device__ __forceinline__ bool zh_touches(const lbm_grid_t& g, const ZouHeArgs& z, const uint8_t* solid, int y, int zz)
+{
+    const int x = z.column;
+    if (solid[((int64_t)zz * g.ny + y) * g.pitch + x]) return false;
+    bool hit = false;
+#pragma unroll
+    for (int j = 1; j < L::Q; ++j) {
+        if (z.sign * L::cx(j) != 1) continue;
+        const int sx = wrap(x - L::cx(j), g.nx), sy = wrap(y - L::cy(j), g.ny);
+        const int sz = L::D == 3 ? wrap(zz - L::cz(j), g.nz) : 0;
+        hit = hit || (sx == z.layer_x && z.layer[(int64_t)sz * g.ny + sy] != 0);
+    }
+    return hit;
+}
+
+// Row of unknown j at cross-section node c: coefficients over s_k and the shifted constant.
+template <class L>
+__device__ __forceinline__ void zh_row(const ZouHeArgs& z, const double* u, double denom, int j, double (&cf)[L::Q],
+                                       double& constant)
+{
+    constexpr int Q = L::Q, D = L::D;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) cf[k] = k == L::opp(j) ? 1.0 : 0.0;
+    double b = 0.0;
+    const double wj = L::w(j);
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const int cja = lat_c<L>(j, a);
+        if (cja == 0) continue;
+        const double s6 = __dmul_rn(__dmul_rn(6.0, wj), (double)cja);
+#pragma unroll
+        for (int k = 0; k < Q; ++k) cf[k] = __dadd_rn(cf[k], __dmul_rn(s6, zh_rho_u_coeff<L>(z, u, denom, a, k)));
+        b = __dadd_rn(b, __dmul_rn(s6, zh_rho_u_const(z, a)));
+    }
+#pragma unroll
+    for (int t = 1; t < D; ++t) {
+        const int cjt = lat_c<L>(j, t);
+        if (cjt == 0) continue;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const double zero_n = z.sign * L::cx(k) == 0 ? 1.0 : 0.0;
+            const double tc = __dsub_rn(__dmul_rn(__dmul_rn(0.5, zero_n), (double)lat_c<L>(k, t)),
+                                        __ddiv_rn(zh_rho_u_coeff<L>(z, u, denom, t, k), 3.0));
+            cf[k] = __dsub_rn(cf[k], __dmul_rn((double)cjt, tc));
+        }
+        b = __dsub_rn(b, __dmul_rn((double)cjt, __ddiv_rn(-zh_rho_u_const(z, t), 3.0)));
+    }
+    double acc = __dmul_rn(cf[0], L::w(0));
+#pragma unroll
+    for (int k = 1; k < Q; ++k) acc = __dadd_rn(acc, __dmul_rn(cf[k], L::w(k)));
+    constant = __dadd_rn(__dsub_rn(b, wj), acc);
+}
+
+// The velocity at cross-section node c (d values) and 1 - sign u_x.
+template <class L>
+__device__ __forceinline__ double zh_velocity(const lbm_grid_t& g, const ZouHeArgs& z, int64_t c, double (&u)[3])
+{
+    const int64_t n = (int64_t)g.ny * g.nz;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) u[a] = (z.velocity != nullptr && a < L::D) ? z.velocity[a * n + c] : 0.0;
+    return __dsub_rn(1.0, __dmul_rn((double)z.sign, u[0]));
+}
+
+// Pass 1: offs[c] = 1 where node c of the column gets rules; the largest
+// number of non-zero coefficients of a rule into offs[n + 1] (atomic max).
+template <class L>
+__global__ void __launch_bounds__(COMPILE_THREADS) zou_he_count_kernel(const lbm_grid_t g, const ZouHeArgs z,
+                                                                       const uint8_t* __restrict__ solid,
+                                                                       int64_t* __restrict__ offs)
+{
+    const int64_t n = (int64_t)g.ny * g.nz;
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int flag = 0, width = 0;
+    if (c < n) {
+        const int y = (int)(c % g.ny), zz = (int)(c / g.ny);
+        if (zh_touches<L>(g, z, solid, y, zz)) {
+            flag = 1;
+            double u[3];
+            const double denom = zh_velocity<L>(g, z, c, u);
+#pragma unroll
+            for (int j = 1; j < L::Q; ++j) {
+                if (z.sign * L::cx(j) != 1) continue;
+                double cf[L::Q], b;
+                zh_row<L>(z, u, denom, j, cf, b);
+                int nz = 0;
+#pragma unroll
+                for (int k = 0; k < L::Q; ++k) nz += cf[k] != 0.0;
+                width = max(width, nz);
+            }
+        }
+        offs[c] = flag;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) width = max(width, __shfl_xor_sync(0xffffffffu, width, off));
+    if ((threadIdx.x & 31) == 0 && width > 0) atomicMax((unsigned long long*)&offs[n + 1], (unsigned long long)width);
+}
+
+// Pass 2: node c's rules at rows offs[c] * n_unknown onwards (unknowns
+// ascending), their non-zero terms packed to the front in ascending k, the
+// rest of the width zero.
+template <class L>
+__global__ void __launch_bounds__(COMPILE_THREADS) zou_he_write_kernel(
+    const lbm_grid_t g, const ZouHeArgs z, const uint8_t* __restrict__ solid, const int64_t* __restrict__ offs,
+    int width, int64_t* __restrict__ node_out, int64_t* __restrict__ dir_out, int64_t* __restrict__ tdir,
+    int64_t* __restrict__ tnode, double* __restrict__ coeff, double* __restrict__ constant)
+{
+    const int64_t n = (int64_t)g.ny * g.nz;
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int x = z.column, y = (int)(c % g.ny), zz = (int)(c / g.ny);
+    if (!zh_touches<L>(g, z, solid, y, zz)) return;
+    double u[3];
+    const double denom = zh_velocity<L>(g, z, c, u);
+    const int64_t flat = ((int64_t)zz * g.ny + y) * g.nx + x;
+    // the streamed population s_k: (k, x - c_k), or (opp k, x) where x - c_k is solid
+    int64_t key_node[L::Q];
+    int key_dir[L::Q];
+#pragma unroll
+    for (int k = 0; k < L::Q; ++k) {
+        const int sx = wrap(x - L::cx(k), g.nx), sy = wrap(y - L::cy(k), g.ny);
+        const int sz = L::D == 3 ? wrap(zz - L::cz(k), g.nz) : 0;
+        const bool blocked = solid[((int64_t)sz * g.ny + sy) * g.pitch + sx] != 0;
+        key_dir[k] = blocked ? L::opp(k) : k;
+        key_node[k] = blocked ? flat : ((int64_t)sz * g.ny + sy) * g.nx + sx;
+    }
+    int n_unknown = 0;
+#pragma unroll
+    for (int j = 1; j < L::Q; ++j) n_unknown += z.sign * L::cx(j) == 1;
+    int64_t row = offs[c] * n_unknown;
+#pragma unroll
+    for (int j = 1; j < L::Q; ++j) {
+        if (z.sign * L::cx(j) != 1) continue;
+        double cf[L::Q], b;
+        zh_row<L>(z, u, denom, j, cf, b);
+        node_out[row] = flat;
+        dir_out[row] = j;
+        constant[row] = b;
+        int p = 0;
+#pragma unroll
+        for (int k = 0; k < L::Q; ++k) {
+            if (cf[k] == 0.0 || p >= width) continue;
+            tdir[row * width + p] = key_dir[k];
+            tnode[row * width + p] = key_node[k];
+            coeff[row * width + p] = cf[k];
+            ++p;
+        }
+        for (; p < width; ++p) {
+            tdir[row * width + p] = 0;
+            tnode[row * width + p] = 0;
+            coeff[row * width + p] = 0.0;
+        }
+        ++row;
+    }
+}
+
+template <class L, int ST>
+int zou_he_count(const lbm_grid_t& g, const ZouHeArgs& z, const uint8_t* solid, int64_t* offs, cudaStream_t s)
+{
+    const int64_t n = (int64_t)g.ny * g.nz;
+    const int64_t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    int64_t* sums = offs + n + 2;
+    if (cudaMemsetAsync(offs + n + 1, 0, sizeof(int64_t), s) != cudaSuccess) return LBM_ERR_LAUNCH;
+    zou_he_count_kernel<L><<<blocks_for(n, COMPILE_THREADS), COMPILE_THREADS, 0, s>>>(g, z, solid, offs);
+    scan_sums_kernel<<<(unsigned)nb, SCAN_BLOCK, 0, s>>>(offs, n, sums);
+    scan_spine_kernel<<<1, SCAN_BLOCK, 0, s>>>(sums, nb);
+    scan_apply_kernel<<<(unsigned)nb, SCAN_BLOCK, 0, s>>>(offs, n, sums, nb);
+    return launch_status();
+}
+
+template <class L, int ST>
+int zou_he_write(const lbm_grid_t& g, const ZouHeArgs& z, const uint8_t* solid, const int64_t* offs, int width,
+                 int64_t* node, int64_t* dir, int64_t* tdir, int64_t* tnode, double* coeff, double* constant,
+                 cudaStream_t s)
+{
+    const int64_t n = (int64_t)g.ny * g.nz;
+    zou_he_write_kernel<L><<<blocks_for(n, COMPILE_THREADS), COMPILE_THREADS, 0, s>>>(g, z, solid, offs, width, node,
+                                                                                     dir, tdir, tnode, coeff, constant);
+    return launch_status();
+}
+
 template <class L, int ST>
 int ball_voxelize(const lbm_grid_t& g, BallArgs b, uint8_t* solid, cudaStream_t s)
 {
@@ -437,4 +670,40 @@ extern "C" int lbm_compile_terms(const lbm_grid_t* g, int32_t layout, const uint
     if (layout == LBM_LAYOUT_AA_EVEN && n > 0 && (!solid || (wall_u && (!coeff || !extra)))) return LBM_ERR_INVALID;
     LBM_DISPATCH(g->lattice, LBM_F64, compile_terms, *g, layout, solid, wall_u, n, direction, node, coeff, slot, extra,
                  (cudaStream_t)stream);
+}
+
+static bool zou_he_ok(const lbm_grid_t* g, const uint8_t* solid, int32_t column, int32_t sign, int32_t layer_x,
+                      const uint8_t* layer)
+{
+    if (!compile_grid_ok(g) || !solid || !layer || (sign != 1 && sign != -1)) return false;
+    return column >= 0 && column < g->nx && layer_x >= 0 && layer_x < g->nx;
+}
+
+extern "C" int64_t lbm_zou_he_scratch(const lbm_grid_t* g)
+{
+    if (!compile_grid_ok(g)) return LBM_ERR_INVALID;
+    const int64_t n = (int64_t)g->ny * g->nz;
+    return n + 2 + (n + SCAN_BLOCK - 1) / SCAN_BLOCK + 1;  // flags, two result words, the scan's block sums
+}
+
+extern "C" int lbm_zou_he_count(const lbm_grid_t* g, const uint8_t* solid, int32_t column, int32_t sign,
+                                int32_t layer_x, const uint8_t* layer, const double* velocity, double rho_out,
+                                int64_t* scratch, lbm_stream_t stream)
+{
+    if (!zou_he_ok(g, solid, column, sign, layer_x, layer) || !scratch) return LBM_ERR_INVALID;
+    const ZouHeArgs z{column, sign, layer_x, layer, velocity, rho_out};
+    LBM_DISPATCH(g->lattice, LBM_F64, zou_he_count, *g, z, solid, scratch, (cudaStream_t)stream);
+}
+
+extern "C" int lbm_zou_he_write(const lbm_grid_t* g, const uint8_t* solid, int32_t column, int32_t sign,
+                                int32_t layer_x, const uint8_t* layer, const double* velocity, double rho_out,
+                                const int64_t* scratch, int32_t width, int64_t* node, int64_t* direction,
+                                int64_t* term_dir, int64_t* term_node, double* coeff, double* constant,
+                                lbm_stream_t stream)
+{
+    if (!zou_he_ok(g, solid, column, sign, layer_x, layer) || !scratch || width < 1) return LBM_ERR_INVALID;
+    if (!node || !direction || !term_dir || !term_node || !coeff || !constant) return LBM_ERR_INVALID;
+    const ZouHeArgs z{column, sign, layer_x, layer, velocity, rho_out};
+    LBM_DISPATCH(g->lattice, LBM_F64, zou_he_write, *g, z, solid, scratch, width, node, direction, term_dir, term_node,
+                 coeff, constant, (cudaStream_t)stream);
 }

@@ -1,8 +1,9 @@
-"""Device-side rule compiler: body voxelisation, wall links and Bouzidi rules built on the GPU.
+"""Device-side rule compiler: body voxelisation, wall links, Bouzidi and Zou-He rules built on the GPU.
 
 The host builders (``geometry.voxelize``, ``geometry.wall_links``,
-``link_rules.bouzidi_rules``; reference ``src/lbm/geometry.py:140-206``,
-``link_rules.py:154-188``) walk every node of the grid in NumPy: for a 256^3
+``link_rules.bouzidi_rules``, ``open_boundaries.open_channel``; reference
+``src/lbm/geometry.py:140-206``, ``link_rules.py:154-188``,
+``open_boundaries.py:96-186``) walk every node of the grid in NumPy: for a 256^3
 duct with a sphere that is tens of seconds of set-up before the first step.
 These functions take the same arguments and return the same objects (host
 NumPy arrays, equal bit for bit: the kernels in ``csrc/compile.cu`` round
@@ -12,7 +13,9 @@ every operation as NumPy does), but do the per-node work on the device:
 * ``wall_links(lattice, body, solid)`` -- ``lbm_ball_links_count`` + ``_write``
   (links grouped by direction, nodes ascending, wall fractions q);
 * ``bouzidi_rules(lattice, links, solid)`` -- ``lbm_bouzidi_links``;
-* ``ball_channel(...)`` -- the three in sequence on one device-resident mask.
+* ``ball_channel(...)`` -- the three in sequence on one device-resident mask;
+* ``open_channel(lattice, solid, inflow, rho_out)`` -- ``lbm_zou_he_count`` +
+  ``_write``: the Zou-He inlet and outlet rules of an open channel.
 
 Bodies are balls (``Ball``: circles and spheres), the body type of the
 reference's builders that the benchmark configurations use.
@@ -157,3 +160,63 @@ def ball_channel(lattice: VelocitySet, body, solid):
     links = WallLinks(node.cpu().numpy(), direction.cpu().numpy().astype(np.int64), q.cpu().numpy())
     rules = LinkRules(x, j, AffineSet.from_dense(tdir, tnode, coeff, np.zeros(x.size)))
     return mask.cpu().numpy().astype(bool).reshape(shape), links, rules
+
+
+def _zou_he_column(torch, lattice, mask, shape, column, sign, layer_x, layer, velocity, rho_out):
+    """Pass 1 of one open column: (grid, scratch, arguments, rule rows, widest rule)."""
+    grid = _grid(lattice, shape)
+    lib = N.load()
+    n_scratch = int(lib.lbm_zou_he_scratch(N.C.byref(grid)))
+    if n_scratch <= 0:
+        raise N.NativeError("lbm_zou_he_scratch: invalid grid")
+    scratch = torch.empty(n_scratch, dtype=torch.int64, device="cuda")
+    plane = _mask_on_device(torch, layer)
+    args = (N.C.byref(grid), N.ptr(mask), column, sign, layer_x, N.ptr(plane), N.ptr(velocity), float(rho_out))
+    N.call("lbm_zou_he_count", *args, N.ptr(scratch), _stream(torch))
+    n = int(np.prod(shape[:-1]))
+    nodes, width = (int(v) for v in scratch[n:n + 2].cpu().tolist())
+    n_unknown = sum(1 for c in lattice.c if sign * c[0] == 1)
+    return (args, scratch, plane), nodes * n_unknown, width
+
+
+def open_channel(lattice: VelocitySet, solid, inflow, rho_out: float = 1.0):
+    """``open_boundaries.open_channel`` on the device: the same closed mask and the same rules --
+    rule order, packed terms, coefficients and constants bit for bit (reference
+    ``open_boundaries.py:96-186``). ``inflow`` broadcasts to (d, *cross_section) and acts at
+    x = 1; ``rho_out`` is imposed at x = nx - 2. One thread per node of each open column
+    (``lbm_zou_he_count`` + ``lbm_zou_he_write``); the x = 0 and x = nx - 1 layers are closed on the
+    host, as ``open_channel`` does."""
+    from .open_boundaries import _layers
+
+    torch = _torch()
+    lattice = as_lattice(lattice)
+    closed, inlet, outlet = _layers(solid)
+    shape = closed.shape
+    if len(shape) != lattice.d:
+        raise ValueError(f"{lattice.name} needs a {lattice.d}D mask, got shape {shape}")
+    nx = shape[-1]
+    mask = _mask_on_device(torch, closed)
+    cross = shape[:-1]
+    vel = np.array(np.broadcast_to(np.asarray(inflow, dtype=np.float64), (lattice.d, *cross)))  # a writable copy
+    velocity = torch.from_numpy(vel.reshape(lattice.d, -1)).to("cuda")
+    columns = [_zou_he_column(torch, lattice, mask, shape, 1, +1, 0, inlet[..., 0], velocity, 1.0),
+               _zou_he_column(torch, lattice, mask, shape, nx - 2, -1, nx - 1, outlet[..., -1], None, rho_out)]
+    rows = sum(r for _, r, _ in columns)
+    width = max([max(w, 1) for _, r, w in columns if r], default=1)
+    node = torch.empty(rows, dtype=torch.int64, device="cuda")
+    direction = torch.empty(rows, dtype=torch.int64, device="cuda")
+    tdir = torch.empty((rows, width), dtype=torch.int64, device="cuda")
+    tnode = torch.empty((rows, width), dtype=torch.int64, device="cuda")
+    coeff = torch.empty((rows, width), dtype=torch.float64, device="cuda")
+    const = torch.empty(rows, dtype=torch.float64, device="cuda")
+    start = 0
+    for (args, scratch, _plane), r, _ in columns:
+        if r:
+            sl = slice(start, start + r)
+            N.call("lbm_zou_he_write", *args, N.ptr(scratch), width, N.ptr(node[sl]), N.ptr(direction[sl]),
+                   N.ptr(tdir[sl]), N.ptr(tnode[sl]), N.ptr(coeff[sl]), N.ptr(const[sl]), _stream(torch))
+        start += r
+    host = lambda t: t.cpu().numpy()  # noqa: E731
+    rules = LinkRules(host(node), host(direction), AffineSet.from_dense(host(tdir), host(tnode), host(coeff),
+                                                                        host(const)))
+    return closed, rules

@@ -52,6 +52,15 @@ def _stream_keys(lattice: VelocitySet, solid_flat, nodes, shape):
     return key_dir, key_node
 
 
+def _weighted_sum(a, key_w):
+    """sum_k a[m, r, k] key_w[m, k], summed over k left to right: one fixed order on every host,
+    which the device-side builder (``csrc/compile.cu``, ``zh_row``) follows."""
+    acc = a[..., 0] * key_w[:, None, 0]
+    for k in range(1, a.shape[-1]):
+        acc = acc + a[..., k] * key_w[:, None, k]
+    return acc
+
+
 def _zou_he_coefficients(lattice, solid, layer_mask, column, sign, velocity=None, rho_out=None, dvel=None):
     """Rules of one open column as dense coefficient arrays.
 
@@ -130,8 +139,8 @@ def _zou_he_coefficients(lattice, solid, layer_mask, column, sign, velocity=None
                 dconst[:, r] -= c[j, t] * dtrans_k[t]
     # Shifted storage f~ = f - w: const_shifted = const - w_j + sum_k a_k w_k
     key_w = w[key_dir]  # (m, q)
-    const = const - w[unknown][None, :] + np.einsum("mrq,mq->mr", coeff, key_w)
-    dconst = dconst + np.einsum("mrq,mq->mr", dcoeff, key_w)
+    const = const - w[unknown][None, :] + _weighted_sum(coeff, key_w)
+    dconst = dconst + _weighted_sum(dcoeff, key_w)
 
     node_out = np.repeat(nodes, unknown.size)
     dir_out = np.tile(unknown, m)

@@ -350,6 +350,31 @@ int lbm_compile_terms(const lbm_grid_t* grid, int32_t layout, const uint8_t* sol
                       const int64_t* direction, const int64_t* node, const double* coeff, int64_t* slot,
                       double* extra, lbm_stream_t stream);
 
+/* Zou-He velocity inlet / density outlet rules of one open column x = column of a
+ * channel whose x = 0 and x = nx - 1 layers are closed -- replaces _zou_he and
+ * open_channel (src/lbm/open_boundaries.py:96-186). solid: the closed mask
+ * (natural order, pitch = nx); layer: (nz * ny) the fluid nodes of the open
+ * layer at x = layer_x before it was closed; sign +1: inlet, velocity (d, nz * ny)
+ * prescribed at the column; sign -1: outlet at density rho_out (velocity NULL).
+ * Node (x, y, z) of the column gets one rule per unknown population j
+ * (sign c_jx = +1, ascending j) when it is fluid and some unknown streams in from
+ * the layer: f_j = b + sum a_m f*_{k_m}(y_m), its non-zero terms over the node's
+ * streamed populations packed to the front in ascending k, b the shifted-storage
+ * constant. Two passes over a scratch of lbm_zou_he_scratch(grid) int64 (n = ny * nz):
+ * lbm_zou_he_count leaves the number of nodes with rules in scratch[n] and the
+ * largest number of terms of a rule in scratch[n + 1]; lbm_zou_he_write (same
+ * arguments and scratch) fills node[rows], direction[rows], term_dir/term_node/
+ * coeff[rows][width] (zero beyond each rule's terms) and constant[rows], rows =
+ * nodes * unknowns, node by node. */
+int64_t lbm_zou_he_scratch(const lbm_grid_t* grid);
+int lbm_zou_he_count(const lbm_grid_t* grid, const uint8_t* solid, int32_t column, int32_t sign, int32_t layer_x,
+                     const uint8_t* layer, const double* velocity, double rho_out, int64_t* scratch,
+                     lbm_stream_t stream);
+int lbm_zou_he_write(const lbm_grid_t* grid, const uint8_t* solid, int32_t column, int32_t sign, int32_t layer_x,
+                     const uint8_t* layer, const double* velocity, double rho_out, const int64_t* scratch,
+                     int32_t width, int64_t* node, int64_t* direction, int64_t* term_dir, int64_t* term_node,
+                     double* coeff, double* constant, lbm_stream_t stream);
+
 /* ---- immersed boundary (direct forcing, multi-direct) ------------------- */
 /* Replaces ImmersedForcing.force_field (src/lbm/ibm.py:189-214). */
 

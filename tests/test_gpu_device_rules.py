@@ -97,3 +97,78 @@ def test_device_compiled_probe_equals_the_host_compiled_slots(backend, dtype):
     np.testing.assert_array_equal(via_device, via_host)
     np.testing.assert_allclose(via_host, probe.weight.T @ gpu.evaluate_affine(probe.compiled(gpu.state_layout)),
                                rtol=1e-12, atol=1e-18)
+
+
+def assert_same_rules(device, host):
+    np.testing.assert_array_equal(device.node, host.node)
+    np.testing.assert_array_equal(device.direction, host.direction)
+    for a, b in ((device.values.direction, host.values.direction), (device.values.node, host.values.node),
+                 (device.values.coeff, host.values.coeff), (device.values.constant, host.values.constant)):
+        assert a.shape == b.shape and a.dtype == b.dtype
+        np.testing.assert_array_equal(a, b)  # bit for bit
+
+
+def _open_cases():
+    """(lattice, solid, inflow, rho_out): channels with walls, bodies at the open columns, a
+    partly closed open layer, a fully periodic cross-section, the cylinder and sphere channels."""
+    out = []
+    for d in (2, 3):
+        p, inflow = cases.open_channel_case(NS, d)
+        nx, ny = 12, 9
+        solid = lbm.channel_walls(nx, ny) if d == 2 else lbm.channel_walls(nx, ny, 5)
+        out.append((f"small{d}d", p.lattice, solid, inflow, 1.003))
+    rng = np.random.default_rng(5)
+    solid = lbm.channel_walls(17, 13, 7)
+    solid[2:4, 3:5, 1] = True       # a block on the inlet column
+    solid[3, 6, 0] = True           # a closed node in the open inlet layer
+    solid[1:3, 2:4, -2] = True      # a block on the outlet column
+    inflow = rng.uniform(-0.02, 0.05, size=(3, 7, 13))
+    out.append(("bodies3d", lbm.D3Q19, solid, inflow, 0.998))
+    solid = np.zeros((11, 10), dtype=bool)  # periodic in y: no walls
+    inflow = rng.uniform(0.0, 0.04, size=(2, 11))
+    out.append(("periodic2d", lbm.D2Q9, solid, inflow, 1.0))
+    solid = np.zeros((5, 6, 4), dtype=bool)  # the narrowest channel (nx = 4), periodic in y and z
+    out.append(("narrow3d", lbm.D3Q19, solid, np.full((3, 5, 6), 0.03), 1.01))
+    ny, nx = 164, 880
+    y = np.arange(ny) - 0.5
+    profile = np.where((y > 0) & (y < ny - 2), 4.0 * 0.05 * y * (ny - 2 - y) / (ny - 2) ** 2, 0.0)
+    solid = np.zeros((ny, nx), dtype=bool)
+    solid[0, :] = solid[-1, :] = True
+    solid |= lbm.voxelize(lbm.circle(200.0, 82.0, 20.0), solid.shape)
+    out.append(("cylinder", lbm.D2Q9, solid, np.stack([profile, np.zeros(ny)]), 1.0))
+    solid = np.zeros((64, 64, 128), dtype=bool)
+    solid[:, [0, -1], :] = True
+    solid[[0, -1], :, :] = True
+    inflow = np.zeros((3, 64, 64))
+    inflow[0, 1:-1, 1:-1] = 0.04
+    out.append(("sphere_channel", lbm.D3Q19, solid, inflow, 1.0))
+    return out
+
+
+@pytest.mark.parametrize("case", _open_cases(), ids=lambda c: c[0])
+def test_device_open_channel_equals_the_host_builder_bit_for_bit(case):
+    _, lattice, solid, inflow, rho_out = case
+    hs, hr = lbm.open_channel(lattice, solid, inflow, rho_out=rho_out)
+    ds, dr = dev.open_channel(lattice, solid, inflow, rho_out=rho_out)
+    np.testing.assert_array_equal(ds, hs)
+    assert len(hr) > 0
+    assert_same_rules(dr, hr)
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_device_open_channel_equals_the_reference_golden_rules(d):
+    ref = golden(f"zouhe{d}d_float64")
+    nx, ny, nz = 12, 9, 5
+    solid = lbm.channel_walls(nx, ny) if d == 2 else lbm.channel_walls(nx, ny, nz)
+    inflow = np.zeros((d, *solid.shape[:-1]))
+    inflow[0], inflow[1] = 0.04, 0.01
+    if d == 3:
+        inflow[2] = -0.02
+    ds, dr = dev.open_channel(lbm.LATTICES["D2Q9" if d == 2 else "D3Q19"], solid, inflow, rho_out=1.003)
+    np.testing.assert_array_equal(ds, ref["solid"])
+    assert_rules_match(dr, ref, "rule_")
+
+
+def test_device_open_channel_rejects_what_the_host_builder_rejects():
+    with pytest.raises(ValueError, match="at least 4 nodes"):
+        dev.open_channel(lbm.D2Q9, np.zeros((6, 3), dtype=bool), 0.01)
