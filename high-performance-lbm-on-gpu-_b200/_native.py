@@ -25,8 +25,9 @@ IBM_FUSED_MAX = 4096
 LBM_D2Q9, LBM_D3Q19 = 0, 1
 LBM_F32, LBM_F64, LBM_F16, LBM_BF16 = 0, 1, 2, 3
 LBM_PULL, LBM_AA_EVEN, LBM_AA_ODD = 0, 1, 2
-COLLIDE_TRT, COLLIDE_REGULARIZED = 0, 1
-COLLISION_CODE = {"bgk": COLLIDE_TRT, "trt": COLLIDE_TRT, "regularized": COLLIDE_REGULARIZED}
+COLLIDE_TRT, COLLIDE_REGULARIZED, COLLIDE_CUMULANT = 0, 1, 2
+COLLISION_CODE = {"bgk": COLLIDE_TRT, "trt": COLLIDE_TRT, "regularized": COLLIDE_REGULARIZED,
+                  "cumulant": COLLIDE_CUMULANT}
 LAYOUT_PULL, LAYOUT_AA_ODD, LAYOUT_AA_EVEN = 0, 1, 2
 KIND_SOLID, KIND_SPECIAL, KIND_NEAR, KIND_EDGE = 1, 2, 4, 8
 LAUNCH_FUSED, LAUNCH_BULK, LAUNCH_BOUNDARY = 0, 1, 2

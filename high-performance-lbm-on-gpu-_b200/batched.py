@@ -52,8 +52,9 @@ class BatchedSolver:
             raise BackendUnavailable(str(exc)) from exc
         if not params_list:
             raise ValueError("a batch needs at least one domain")
-        if any(getattr(p, "collision", "bgk") == "regularized" for p in params_list):
-            raise ValueError("the batched step runs TRT/BGK collision only; use CudaSolver for 'regularized'")
+        if any(getattr(p, "collision", "bgk") in ("regularized", "cumulant") for p in params_list):
+            raise ValueError("the batched step runs TRT/BGK collision only; use CudaSolver for 'regularized' "
+                             "and 'cumulant'")
         self.torch = torch
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         self.params = list(params_list)

@@ -82,7 +82,10 @@ int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lb
     a.force_field = p->force_field;
     a.nbr = p->solid_nbr;
     if (!a.nbr) return LBM_ERR_INVALID;
-    if (p->collision != LBM_COLLIDE_TRT && p->collision != LBM_COLLIDE_REGULARIZED) return LBM_ERR_INVALID;
+    if (p->collision != LBM_COLLIDE_TRT && p->collision != LBM_COLLIDE_REGULARIZED &&
+        p->collision != LBM_COLLIDE_CUMULANT)
+        return LBM_ERR_INVALID;
+    if (p->collision == LBM_COLLIDE_CUMULANT && g->lattice != LBM_D2Q9) return LBM_ERR_UNSUPPORTED;
     a.collision = p->collision;
     // 16-bit storage rounds stochastically and needs the step counter
     const bool half = g->storage == LBM_F16 || g->storage == LBM_BF16;

@@ -751,6 +751,10 @@ int ibm_step(const StepArgs& a, const lbm_grid_t& g, const lbm_physics_t& p, con
 {
     if (a.collision == LBM_COLLIDE_REGULARIZED)
         return ibm_step_model<L, ST, LBM_COLLIDE_REGULARIZED>(a, g, p, ib, iterations, force, s);
+    if (a.collision == LBM_COLLIDE_CUMULANT) {
+        if constexpr (L::D == 2) return ibm_step_model<L, ST, LBM_COLLIDE_CUMULANT>(a, g, p, ib, iterations, force, s);
+        return LBM_ERR_UNSUPPORTED;
+    }
     return ibm_step_model<L, ST, LBM_COLLIDE_TRT>(a, g, p, ib, iterations, force, s);
 }
 

@@ -221,6 +221,8 @@ __device__ __forceinline__ double v_sub(double a, double b) { return __dsub_rn(a
 __device__ __forceinline__ double v_mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double v_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ double v_rcp(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float v_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double v_div(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float v_neg(float a) { return -a; }
 __device__ __forceinline__ double v_neg(double a) { return -a; }
 // Two nodes at once on the packed FP32x2 pipe (FFMA2/FADD2/FMUL2): each lane
@@ -598,12 +600,112 @@ __device__ __forceinline__ void collide_regularized(R (&f)[L::Q], const Relax<R>
     }
 }
 
-// The node update of collision model CM (LBM_COLLIDE_*): TRT/BGK or regularised.
+// ---------------------------------------------------------------- cumulant collision (D2Q9)
+// The cumulant method (M. Geier, M. Schoenherr, A. Pasquali, M. Krafczyk,
+// Comput. Math. Appl. 70 (2015) 507-547: central moments by the 'chimera'
+// transformation, sec. 3; forcing by the half-force velocity shift, sec. 2.4)
+// on the tensor-product lattice D2Q9, whose populations carry the moments
+// (m, n), m, n <= 2. About u = (j + F/2)/rho: k20 - k02 and k11 relax with w+,
+// k20 + k02 -> 2 rho/3, k21, k12 -> 0, the fourth-order cumulant
+// k22/rho - (k20 k02 + 2 k11^2)/rho^2 -> 0, k10, k01 mirrored (the force).
+// Evaluated in deviations only, so round-off stays at the scale of the
+// shifted populations: k~ are the central moments of f~ = f - w (chimera along
+// x, then y); those of the weights are M_m(u_x) M_n(u_y), M = (1, -u, 1/3 + u^2),
+// and each post-collision moment is formed directly as its difference from the
+// weights' one, p = k* - M M:
+//   p00 = drho, p10 = 2 u_x - k~10, p01 = 2 u_y - k~01,
+//   D* = (1 - w+) ((k~20 - k~02) + (u_x^2 - u_y^2)), k11* = (1 - w+) (k~11 + u_x u_y),
+//   a = drho/3 + D*/2, b = drho/3 - D*/2, p20 = a - u_x^2, p02 = b - u_y^2, p11 = k11* - u_x u_y,
+//   p21 = u_y (1/3 + u_x^2), p12 = u_x (1/3 + u_y^2),
+//   p22 = (drho/9 + a b + 2 k11*^2)/rho - (u_x^2 + u_y^2)/3 - u_x^2 u_y^2,
+// then the inverse chimera along y, then x. Plain rounded operations (no
+// fused multiply-add) in the order of the oracle's restatement, so a step
+// without boundaries gives the oracle's bits. Used with the one-node kernels
+// (SCALE_LOG2 = 0).
+template <class R>
+__device__ __forceinline__ void chimera(R am, R a0, R ap, R u, R& k0, R& k1, R& k2)
+{
+    k0 = v_add(v_add(am, a0), ap);
+    const R s = v_sub(ap, am);
+    k1 = v_sub(s, v_mul(u, k0));
+    k2 = v_add(v_sub(v_add(ap, am), v_mul(v_mul(R(2), u), s)), v_mul(v_mul(u, u), k0));
+}
+
+template <class R>
+__device__ __forceinline__ void chimera_inverse(R k0, R k1, R k2, R u, R& am, R& a0, R& ap)
+{
+    const R s = v_add(k1, v_mul(u, k0));
+    const R p = v_sub(v_add(k2, v_mul(v_mul(R(2), u), s)), v_mul(v_mul(u, u), k0));
+    am = v_mul(R(0.5), v_sub(p, s));
+    a0 = v_sub(k0, p);
+    ap = v_mul(R(0.5), v_add(p, s));
+}
+
+// The D2Q9 slot of direction (cx, cy).
+template <class L>
+__host__ __device__ constexpr int slot_of(int cx, int cy)
+{
+    int k = 0;
+    for (int i = 0; i < L::Q; ++i)
+        if (L::cx(i) == cx && L::cy(i) == cy) k = i;
+    return k;
+}
+
+template <class L, class R>
+__device__ __forceinline__ void collide_cumulant(R (&f)[L::Q], const Relax<R>& c, R Fx, R Fy)
+{
+    static_assert(L::D == 2 && L::Q == 9, "the cumulant collision is built for D2Q9");
+    R drho = f[0], jx = R(0), jy = R(0);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) drho = v_add(drho, f[i]);
+    // momentum over the directions in slot order, as the oracle sums it
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        if (L::cx(i)) jx = L::cx(i) > 0 ? v_add(jx, f[i]) : v_sub(jx, f[i]);
+        if (L::cy(i)) jy = L::cy(i) > 0 ? v_add(jy, f[i]) : v_sub(jy, f[i]);
+    }
+    const R rho = v_add(R(1), drho);
+    const R ux = v_div(v_add(jx, v_mul(R(0.5), Fx)), rho);
+    const R uy = v_div(v_add(jy, v_mul(R(0.5), Fy)), rho);
+    R t0[3], t1[3], t2[3];  // along x, per row cy = -1, 0, 1
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        chimera(f[slot_of<L>(-1, r - 1)], f[slot_of<L>(0, r - 1)], f[slot_of<L>(1, r - 1)], ux, t0[r], t1[r], t2[r]);
+    R k[3][3];
+    chimera(t0[0], t0[1], t0[2], uy, k[0][0], k[0][1], k[0][2]);
+    chimera(t1[0], t1[1], t1[2], uy, k[1][0], k[1][1], k[1][2]);
+    chimera(t2[0], t2[1], t2[2], uy, k[2][0], k[2][1], k[2][2]);
+    const R third = R(1.0 / 3.0);
+    const R uxx = v_mul(ux, ux), uyy = v_mul(uy, uy), uxy = v_mul(ux, uy);
+    const R keep = v_sub(R(1), c.wp);
+    const R dev = v_mul(keep, v_add(v_sub(k[2][0], k[0][2]), v_sub(uxx, uyy)));
+    const R k11 = v_mul(keep, v_add(k[1][1], uxy));
+    const R d3 = v_mul(drho, third);
+    const R a = v_add(d3, v_mul(R(0.5), dev));
+    const R b = v_sub(d3, v_mul(R(0.5), dev));
+    const R x = v_add(v_add(v_mul(drho, R(1.0 / 9.0)), v_mul(a, b)), v_mul(R(2), v_mul(k11, k11)));
+    const R p22 = v_sub(v_sub(v_div(x, rho), v_mul(v_add(uxx, uyy), third)), v_mul(uxx, uyy));
+    const R p[3][3] = {{drho, v_sub(v_mul(R(2), uy), k[0][1]), v_sub(b, uyy)},
+                       {v_sub(v_mul(R(2), ux), k[1][0]), v_sub(k11, uxy), v_mul(ux, v_add(third, uyy))},
+                       {v_sub(a, uxx), v_mul(uy, v_add(third, uxx)), p22}};
+    R q0[3], q1[3], q2[3];  // q_m[r]: moment m along x of row r
+    chimera_inverse(p[0][0], p[0][1], p[0][2], uy, q0[0], q0[1], q0[2]);
+    chimera_inverse(p[1][0], p[1][1], p[1][2], uy, q1[0], q1[1], q1[2]);
+    chimera_inverse(p[2][0], p[2][1], p[2][2], uy, q2[0], q2[1], q2[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        chimera_inverse(q0[r], q1[r], q2[r], ux, f[slot_of<L>(-1, r - 1)], f[slot_of<L>(0, r - 1)],
+                        f[slot_of<L>(1, r - 1)]);
+}
+
+// The node update of collision model CM (LBM_COLLIDE_*): TRT/BGK, regularised or cumulant.
 template <class L, class R, int CM>
 __device__ __forceinline__ void collide_model(R (&f)[L::Q], const Relax<R>& c, bool uniform, R Fx, R Fy, R Fz)
 {
     if constexpr (CM == LBM_COLLIDE_REGULARIZED)
         collide_regularized<L, R>(f, c, Fx, Fy, Fz);
+    else if constexpr (CM == LBM_COLLIDE_CUMULANT && L::D == 2)
+        collide_cumulant<L, R>(f, c, Fx, Fy);
     else
         collide_node<L, R>(f, c, uniform, Fx, Fy, Fz);
 }

@@ -842,6 +842,17 @@ int launch_step(const StepArgs& a, int variant, int mode, int tile_x, int tile_y
         default: return LBM_ERR_INVALID;
         }
     }
+    if (a.collision == LBM_COLLIDE_CUMULANT) {
+        if constexpr (L::D == 2) {
+            switch (variant) {
+            case LBM_PULL: return launch_mode<L, ST, LBM_PULL, LBM_COLLIDE_CUMULANT>(a, mode, tile_x, tile_y, stream);
+            case LBM_AA_EVEN: return launch_mode<L, ST, LBM_AA_EVEN, LBM_COLLIDE_CUMULANT>(a, mode, tile_x, tile_y, stream);
+            case LBM_AA_ODD: return launch_mode<L, ST, LBM_AA_ODD, LBM_COLLIDE_CUMULANT>(a, mode, tile_x, tile_y, stream);
+            default: return LBM_ERR_INVALID;
+            }
+        }
+        return LBM_ERR_UNSUPPORTED;  // D2Q9 only
+    }
     if (a.collision != LBM_COLLIDE_TRT) return LBM_ERR_INVALID;
     switch (variant) {
     case LBM_PULL: return launch_mode<L, ST, LBM_PULL>(a, mode, tile_x, tile_y, stream);

@@ -19,10 +19,11 @@ import numpy as np
 from .lattice import LATTICES, VelocitySet, as_lattice, default_lattice
 
 TAU_WARNING = 0.51
-COLLISION_MODELS = ("bgk", "trt", "regularized")
-"""The reference's two models and "regularized" (projective regularisation of the non-equilibrium
-part, Latt & Chopard 2006, with one relaxation rate 1/tau), which the reference lists on its
-roadmap (item 3, high Reynolds numbers) but does not implement."""
+COLLISION_MODELS = ("bgk", "trt", "regularized", "cumulant")
+"""The reference's two models, "regularized" (projective regularisation of the non-equilibrium
+part, Latt & Chopard 2006, with one relaxation rate 1/tau) and "cumulant" (the cumulant method of
+Geier et al. 2015 on D2Q9: shear rate 1/tau, bulk and higher-order rates 1), which the reference
+lists on its roadmap (item 3, high Reynolds numbers) but does not implement."""
 SUPPORTED_DTYPES = ("float32", "float64", "float16", "bfloat16")
 COMPUTE_DTYPE = {"float32": "float32", "float64": "float64", "float16": "float32", "bfloat16": "float32"}
 """Arithmetic type of each storage format: 16-bit storage computes in float32."""
@@ -81,7 +82,7 @@ class SimulationParams:
         """Validate and freeze. The checks, their order and their error messages are the
         reference's (``params.py:129-175``) statement for statement, on purpose: they are the
         drop-in's input contract, pinned by ``tests/test_builders_golden.py``. The additions are
-        the 16-bit storage formats and the ``"regularized"`` collision model."""
+        the 16-bit storage formats and the ``"regularized"`` and ``"cumulant"`` collision models."""
         sizes = {"nx": self.nx, "ny": self.ny} | ({} if self.nz is None else {"nz": self.nz})
         if any(n <= 0 for n in sizes.values()):
             got = ", ".join(f"{k}={v}" for k, v in sizes.items())
@@ -106,6 +107,9 @@ class SimulationParams:
                 f"lattice {lattice.name} is {lattice.d}D but the grid is {d}D "
                 "(set nz for 3D, leave it unset for 2D)"
             )
+        if self.collision == "cumulant" and lattice.name != "D2Q9":
+            raise ValueError(f"the cumulant collision is built for D2Q9 (a tensor-product lattice holding "
+                             f"every moment it relaxes); got {lattice.name}")
         shape = (self.ny, self.nx) if d == 2 else (self.nz, self.ny, self.nx)
 
         solid = np.zeros(shape, dtype=bool) if self.solid is None else np.asarray(self.solid)
@@ -157,6 +161,6 @@ class SimulationParams:
     def relaxation_rates(self) -> tuple[float, float]:
         """(omega_plus, omega_minus): 1/tau and 1/(1/2 + Lambda/(tau - 1/2)); equal for BGK."""
         omega_plus = 1.0 / self.tau
-        if self.collision in ("bgk", "regularized"):
+        if self.collision in ("bgk", "regularized", "cumulant"):
             return omega_plus, omega_plus
         return omega_plus, 1.0 / (0.5 + self.magic / (self.tau - 0.5))

@@ -42,8 +42,14 @@ enum { LBM_PULL = 0, LBM_AA_EVEN = 1, LBM_AA_ODD = 2 };
  * second-order Hermite moments (Latt & Chopard 2006) before a single-rate
  * relaxation with omega_plus, Guo forcing -- not in the reference (its roadmap
  * item 3, README "High Reynolds numbers"); the one-node kernels run it
- * whatever the storage, the adjoint and batched steps take TRT only. */
-enum { LBM_COLLIDE_TRT = 0, LBM_COLLIDE_REGULARIZED = 1 };
+ * whatever the storage, the adjoint and batched steps take TRT only.
+ * CUMULANT (D2Q9 only): the cumulant method (Geier et al. 2015) on the
+ * tensor-product lattice -- central moments about u = (j + F/2)/rho by the
+ * chimera transformation, shear moments relaxed with omega_plus, bulk,
+ * third-order and the fourth-order cumulant relaxed with rate 1, first-order
+ * moments mirrored (the force); also one-node kernels only, not in the adjoint
+ * or batched steps; LBM_ERR_UNSUPPORTED on D3Q19. */
+enum { LBM_COLLIDE_TRT = 0, LBM_COLLIDE_REGULARIZED = 1, LBM_COLLIDE_CUMULANT = 2 };
 /* Where a stored state keeps f*_k(y) (reference src/lbm/link_rules.py:16-25). */
 enum { LBM_LAYOUT_PULL = 0, LBM_LAYOUT_AA_ODD = 1, LBM_LAYOUT_AA_EVEN = 2 };
 /* Node kind bits (one byte per node): SOLID; SPECIAL (updated by the boundary

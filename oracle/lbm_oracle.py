@@ -204,6 +204,92 @@ def collide_regularized(lattice, f, wp, force):
     return np.stack(out).astype(f.dtype)
 
 
+def _chimera(am, a0, ap, u):
+    """Central moments of orders 0, 1, 2 along one axis of the three populations with c = -1, 0, +1,
+    about velocity u (the 'chimera' transformation of the cumulant method)."""
+    k0 = (am + a0) + ap
+    s = ap - am
+    k1 = s - u * k0
+    k2 = ((ap + am) - (2.0 * u) * s) + (u * u) * k0
+    return k0, k1, k2
+
+
+def _chimera_inverse(k0, k1, k2, u):
+    """The populations (c = -1, 0, +1) of central moments (k0, k1, k2) about u."""
+    s = k1 + u * k0
+    p = (k2 + (2.0 * u) * s) - (u * u) * k0
+    return 0.5 * (p - s), k0 - p, 0.5 * (p + s)
+
+
+def collide_cumulant(lattice, f, wp, force):
+    """Cumulant collision on every node of f (9, ...), D2Q9 only.
+
+    Not in the reference (its roadmap item 3, README "High Reynolds numbers");
+    restated from the published method: the cumulant lattice Boltzmann
+    equation, M. Geier, M. Schoenherr, A. Pasquali, M. Krafczyk, Comput. Math.
+    Appl. 70 (2015) 507-547 (its central-moment 'chimera' transformation,
+    sec. 3, and forcing by the half-force velocity shift, sec. 2.4), written for
+    the 2D tensor-product lattice D2Q9, whose nine populations carry the
+    nine moments of orders (m, n), m, n <= 2. With u = (j + F/2)/rho and the
+    central moments k_mn = sum_i f_i (c_ix - u_x)^m (c_iy - u_y)^n:
+
+    * second order: k20 - k02 and k11 relax with wp (shear viscosity
+      (1/wp - 1/2)/3), k20 + k02 is set to its equilibrium 2 rho/3 (bulk rate 1);
+    * third order k21, k12 -> 0 and the fourth-order cumulant
+      C22 = k22/rho - (k20 k02 + 2 k11^2)/rho^2 -> 0 (rates 1), so k22* = (k20* k02* + 2 k11*^2)/rho;
+    * first order mirrored, k10* = -k10 (= F_x/2: the post-collision momentum is j + F).
+
+    The cumulant relations use the second-order central moments about u (the
+    first-order ones, -F/2, enter at O(F^2), as in the published scheme).
+
+    Evaluated on shifted populations f~ = f - w, in deviations only, so that
+    round-off stays at the scale of f~ (as in the TRT form): the chimera
+    transformation along x then y gives the central moments k~ of f~ about u;
+    those of the weights are M_m(u_x) M_n(u_y), M = (1, -u, 1/3 + u^2)
+    (w_ij = W_i W_j, W = (1/6, 2/3, 1/6)), and every post-collision moment is
+    written directly as its difference from the weights' one, p = k* - M M:
+        p00 = drho, p10 = 2 u_x - k~10, p01 = 2 u_y - k~01,
+        D* = (1 - wp) ((k~20 - k~02) + (u_x^2 - u_y^2)), k11* = (1 - wp) (k~11 + u_x u_y),
+        a = drho/3 + D*/2, b = drho/3 - D*/2,
+        p20 = a - u_x^2, p02 = b - u_y^2, p11 = k11* - u_x u_y,
+        p21 = u_y (1/3 + u_x^2), p12 = u_x (1/3 + u_y^2),
+        p22 = (drho/9 + a b + 2 k11*^2)/rho - (u_x^2 + u_y^2)/3 - u_x^2 u_y^2;
+    then the inverse chimera along y, then x.
+    """
+    if lattice.q != 9:
+        raise ValueError("the cumulant collision is built for D2Q9")
+    c = lattice.c
+    index = {tuple(ci): i for i, ci in enumerate(c)}
+    dt = f.dtype.type
+    drho = f.sum(axis=0)
+    rho = dt(1.0) + drho
+    jx, jy = _momentum(lattice, f)
+    ux = (jx + 0.5 * force[0]) / rho
+    uy = (jy + 0.5 * force[1]) / rho
+    # along x, per row cy = -1, 0, 1; then along y: k[m][n]
+    rows = [_chimera(f[index[(-1, cy)]], f[index[(0, cy)]], f[index[(1, cy)]], ux) for cy in (-1, 0, 1)]
+    k = [_chimera(rows[0][m], rows[1][m], rows[2][m], uy) for m in range(3)]
+    third = dt(1.0 / 3.0)
+    uxx, uyy, uxy = ux * ux, uy * uy, ux * uy
+    keep = dt(1.0) - dt(wp)
+    dev = keep * ((k[2][0] - k[0][2]) + (uxx - uyy))
+    k11 = keep * (k[1][1] + uxy)
+    d3 = drho * third
+    a = d3 + dt(0.5) * dev
+    b = d3 - dt(0.5) * dev
+    x = (drho * dt(1.0 / 9.0) + a * b) + dt(2.0) * (k11 * k11)
+    p22 = (x / rho - (uxx + uyy) * third) - uxx * uyy
+    post = [[drho, dt(2.0) * uy - k[0][1], b - uyy],
+            [dt(2.0) * ux - k[1][0], k11 - uxy, ux * (third + uyy)],
+            [a - uxx, uy * (third + uxx), p22]]
+    cols = [_chimera_inverse(post[m][0], post[m][1], post[m][2], uy) for m in range(3)]  # cols[m][b]
+    out = np.empty_like(f)
+    for r, cy in enumerate((-1, 0, 1)):
+        am, a0, ap = _chimera_inverse(cols[0][r], cols[1][r], cols[2][r], ux)
+        out[index[(-1, cy)]], out[index[(0, cy)]], out[index[(1, cy)]] = am, a0, ap
+    return out
+
+
 def stream_pull(lattice, f):
     """f_i(x) = f*_i(x - c_i), periodic (``streaming.py:32-37``)."""
     axes = tuple(range(lattice.d))
@@ -392,8 +478,11 @@ class OracleSolver:
             target, slots, coeff, const = self.rules
             values = const + (coeff * f.reshape(-1)[slots]).sum(axis=1)
             streamed.reshape(-1)[target] = values
-        if getattr(self.params, "collision", "bgk") == "regularized":
+        model = getattr(self.params, "collision", "bgk")
+        if model == "regularized":
             post = collide_regularized(lattice, streamed, self.rates[0], force)
+        elif model == "cumulant":
+            post = collide_cumulant(lattice, streamed, self.rates[0], force)
         else:
             post = collide(lattice, streamed, self.rates[0], self.rates[1], force)
         self.f = stochastic_round(np.where(self.fluid, post, f), self.dtype, self.round_step)
