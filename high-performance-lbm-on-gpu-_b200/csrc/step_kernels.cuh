@@ -610,8 +610,21 @@ __global__ void __launch_bounds__(256) lbm_bulk_vec_aa_kernel(const StepArgs a)
 // rows run the one-node path (bulk_node). Same bits as the one-node kernel.
 // In place is safe: slot i of row (y + c_y, z + c_z) is read, in this half,
 // only by the nodes of row (y, z) -- this block -- before the block's barrier.
+// With the TRT collision, a bound on the registers keeps more rows' loads in
+// flight than ptxas's own choice (the one-node fallback spills a little):
+// 4-byte storage six 256-thread blocks per SM (40 registers; ptxas alone: 64,
+// four blocks), 39.8 against 37.4 GLUPS for the AA pair on the 256^3 duct
+// (seven blocks, 32 registers: slower); 8-byte storage three blocks
+// (80 registers; alone: 102, two blocks), 21.4 against 19.9 GLUPS.
+template <int ST, int CM>
+constexpr int odd_rows_min_blocks()
+{
+    if (CM != LBM_COLLIDE_TRT) return 0;
+    return sizeof(typename Storage<ST>::T) == 4 ? 6 : 3;
+}
+
 template <class L, int ST, int CM>
-__global__ void __launch_bounds__(256) lbm_aa_odd_rows_kernel(const StepArgs a)
+__global__ void __launch_bounds__(256, odd_rows_min_blocks<ST, CM>()) lbm_aa_odd_rows_kernel(const StepArgs a)
 {
     using S = Storage<ST>;
     using T = typename S::T;
