@@ -635,7 +635,8 @@ def kernels_study(lbm, torch):
     the per-family ncu launch list (``ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,
     dram__bytes_write.sum``). Families: the 16-bit node-pair fallbacks (nx = 200, pull and AA);
     on a 192^3 float32 duct the checked step (state check fused), the separate scan, the
-    macroscopic readout and the regularised step; the per-pass immersed boundary of a large body
+    macroscopic readout and the regularised step; on a D2Q9 2048^2 periodic grid the TRT and the cumulant
+    steps; the device Zou-He builder on a 256^3 open channel; the per-pass immersed boundary of a large body
     (sphere r = 20, 5 027 markers); the immersed-body adjoint (3D channel); the device-side rule
     compiler on a 256^3 duct with a sphere of radius 40."""
     import dataclasses
@@ -677,6 +678,18 @@ def kernels_study(lbm, torch):
     out["regularized_step_us"] = timed(lambda: s._advance(1))
     del s
     torch.cuda.empty_cache()
+    # D2Q9 2048^2 periodic, float32 (2 x 151 MB lattices, above L2): TRT against the cumulant model
+    p2 = cases.tgv(NS, n=2048, dtype="float32", tau=0.56)[0]
+    for model in ("trt", "cumulant"):
+        s = lbm.make_solver(dataclasses.replace(p2, collision=model), backend="cuda-naive", graph=False)
+        out[f"d2q9_2048_{model}_step_us"] = timed(lambda: s._advance(1))
+        del s
+    torch.cuda.empty_cache()
+    # the device Zou-He builder on a 256^3 open channel (both columns: count, scan, write)
+    solid = lbm.duct_walls(256, 256, 256)
+    inflow = np.zeros((3, 256, 256))
+    inflow[0, 1:-1, 1:-1] = 0.04
+    out["device_zou_he_256_ms"] = timed(lambda: device_rules.open_channel(lbm.D3Q19, solid, inflow), 2) / 1e3
     solid = lbm.duct_walls(96, 64, 64)
     body = lbm.ImmersedBoundary.from_ball(lbm.sphere(40.0, 31.5, 31.5, 20.0), spacing=1.0, iterations=3)
     p = lbm.SimulationParams(nx=96, ny=64, nz=64, tau=0.7, collision="trt", solid=solid, force=(1e-6, 0, 0),
