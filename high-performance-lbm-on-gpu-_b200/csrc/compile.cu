@@ -672,10 +672,12 @@ extern "C" int lbm_compile_terms(const lbm_grid_t* g, int32_t layout, const uint
                  (cudaStream_t)stream);
 }
 
+// An inlet (sign +1) takes its velocity field, an outlet (sign -1) none.
 static bool zou_he_ok(const lbm_grid_t* g, const uint8_t* solid, int32_t column, int32_t sign, int32_t layer_x,
-                      const uint8_t* layer)
+                      const uint8_t* layer, const double* velocity)
 {
     if (!compile_grid_ok(g) || !solid || !layer || (sign != 1 && sign != -1)) return false;
+    if ((sign == 1) != (velocity != nullptr)) return false;
     return column >= 0 && column < g->nx && layer_x >= 0 && layer_x < g->nx;
 }
 
@@ -690,7 +692,7 @@ extern "C" int lbm_zou_he_count(const lbm_grid_t* g, const uint8_t* solid, int32
                                 int32_t layer_x, const uint8_t* layer, const double* velocity, double rho_out,
                                 int64_t* scratch, lbm_stream_t stream)
 {
-    if (!zou_he_ok(g, solid, column, sign, layer_x, layer) || !scratch) return LBM_ERR_INVALID;
+    if (!zou_he_ok(g, solid, column, sign, layer_x, layer, velocity) || !scratch) return LBM_ERR_INVALID;
     const ZouHeArgs z{column, sign, layer_x, layer, velocity, rho_out};
     LBM_DISPATCH(g->lattice, LBM_F64, zou_he_count, *g, z, solid, scratch, (cudaStream_t)stream);
 }
@@ -701,7 +703,7 @@ extern "C" int lbm_zou_he_write(const lbm_grid_t* g, const uint8_t* solid, int32
                                 int64_t* term_dir, int64_t* term_node, double* coeff, double* constant,
                                 lbm_stream_t stream)
 {
-    if (!zou_he_ok(g, solid, column, sign, layer_x, layer) || !scratch || width < 1) return LBM_ERR_INVALID;
+    if (!zou_he_ok(g, solid, column, sign, layer_x, layer, velocity) || !scratch || width < 1) return LBM_ERR_INVALID;
     if (!node || !direction || !term_dir || !term_node || !coeff || !constant) return LBM_ERR_INVALID;
     const ZouHeArgs z{column, sign, layer_x, layer, velocity, rho_out};
     LBM_DISPATCH(g->lattice, LBM_F64, zou_he_write, *g, z, solid, scratch, width, node, direction, term_dir, term_node,

@@ -361,7 +361,8 @@ int lbm_compile_terms(const lbm_grid_t* grid, int32_t layout, const uint8_t* sol
  * open_channel (src/lbm/open_boundaries.py:96-186). solid: the closed mask
  * (natural order, pitch = nx); layer: (nz * ny) the fluid nodes of the open
  * layer at x = layer_x before it was closed; sign +1: inlet, velocity (d, nz * ny)
- * prescribed at the column; sign -1: outlet at density rho_out (velocity NULL).
+ * prescribed at the column; sign -1: outlet at density rho_out (velocity NULL;
+ * LBM_ERR_INVALID for an inlet without a velocity or an outlet with one).
  * Node (x, y, z) of the column gets one rule per unknown population j
  * (sign c_jx = +1, ascending j) when it is fluid and some unknown streams in from
  * the layer: f_j = b + sum a_m f*_{k_m}(y_m), its non-zero terms over the node's

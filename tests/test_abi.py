@@ -99,3 +99,31 @@ def test_checked_step_partial_count_without_a_gpu():
     assert lib.lbm_health_partials(ctypes.byref(grid), ctypes.byref(sp), ctypes.byref(fused)) == 2 * 5 * 17
     bad = N.Launch(48, 4, N.LAUNCH_BULK)
     assert lib.lbm_health_partials(ctypes.byref(grid), ctypes.byref(sp), ctypes.byref(bad)) == N.LBM_ERR_INVALID
+
+
+@pytest.mark.parametrize("change", ["grid", "solid", "layer", "sign", "column", "layer_x", "inlet_without_velocity",
+                                    "outlet_with_velocity", "scratch"])
+def test_zou_he_builder_rejects_invalid_arguments_without_a_gpu(change):
+    """Every rejection returns before any CUDA call, so it runs on a machine without a GPU."""
+    lib = N.load()
+    grid = N.Grid(N.LBM_D3Q19, N.LBM_F64, 12, 9, 5, 12, 12 * 9 * 5)
+    if change == "grid":
+        grid = N.Grid(N.LBM_D3Q19, N.LBM_F64, 12, 9, 5, 11, 12 * 9 * 5)  # pitch < nx
+    one = ctypes.c_void_p(16)  # stands in for a device pointer; never dereferenced on these paths
+    args = {"solid": one, "column": 1, "sign": 1, "layer_x": 0, "layer": one, "velocity": one, "scratch": one}
+    if change in ("solid", "layer", "scratch"):
+        args[change] = None
+    if change == "sign":
+        args["sign"] = 0
+    if change == "column":
+        args["column"] = 12
+    if change == "layer_x":
+        args["layer_x"] = -1
+    if change == "inlet_without_velocity":
+        args["velocity"] = None
+    if change == "outlet_with_velocity":
+        args["sign"] = -1
+    a = args
+    common = (ctypes.byref(grid), a["solid"], a["column"], a["sign"], a["layer_x"], a["layer"], a["velocity"], 1.0)
+    assert lib.lbm_zou_he_count(*common, a["scratch"], None) == N.LBM_ERR_INVALID
+    assert lib.lbm_zou_he_write(*common, a["scratch"], 14, one, one, one, one, one, one, None) == N.LBM_ERR_INVALID
