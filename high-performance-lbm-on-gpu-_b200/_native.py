@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liblbm_b200.so"
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 LBM_OK, LBM_ERR_INVALID, LBM_ERR_UNSUPPORTED, LBM_ERR_LAUNCH, LBM_ERR_TOO_LARGE = 0, -1, -2, -3, -4
 AFFINE_REDUCE_STATIC_MAX_ROWS = 1048576
@@ -71,7 +71,7 @@ class Special(C.Structure):
 
 
 class Health(C.Structure):
-    _fields_ = [("words", vp), ("partial", vp), ("n_partial", i64)]
+    _fields_ = [("words", vp), ("partial", vp), ("n_partial", i64), ("rho", vp), ("u", vp)]
 
 
 class Launch(C.Structure):

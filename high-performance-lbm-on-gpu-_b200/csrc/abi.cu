@@ -94,6 +94,8 @@ int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lb
     a.parity = 0;
     a.health_words = nullptr;
     a.health_partial = nullptr;
+    a.readout_rho = nullptr;
+    a.readout_u = nullptr;
     a.health_slot0 = 0;
     a.wait_limit = WAIT_LIMIT_DEFAULT;
     if (launch && launch->tma_wait_limit) a.wait_limit = launch->tma_wait_limit == LBM_TMA_WAIT_NONE ? 0u : launch->tma_wait_limit;
@@ -106,6 +108,9 @@ int make_args(StepArgs& a, const lbm_grid_t* g, const lbm_physics_t* p, const lb
         if (!h->words || !h->partial || h->n_partial != health_partials(g, sp, tx, ty, mode)) return LBM_ERR_INVALID;
         a.health_words = h->words;
         a.health_partial = h->partial;
+        if ((h->rho == nullptr) != (h->u == nullptr)) return LBM_ERR_INVALID;
+        a.readout_rho = h->rho;
+        a.readout_u = h->u;
     }
     // collision constants, computed once per launch
     a.guo_const = true;
@@ -183,4 +188,4 @@ extern "C" int lbm_kernel_resources(int32_t lattice, int32_t storage, int32_t wh
 
 extern "C" const char* lbm_last_cuda_error(void) { return g_last_error; }
 
-extern "C" int32_t lbm_abi_version(void) { return 8; }
+extern "C" int32_t lbm_abi_version(void) { return 9; }

@@ -175,19 +175,9 @@ __global__ void macro_kernel(const lbm_grid_t g, const lbm_physics_t p, const ui
         for (int a = 0; a < L::D; ++a) u_out[a * qs + nd] = R(0);
         return;
     }
-    R f0 = Storage<ST>::load(f + natural_slot<L>(0, layout) * qs + nd);
-    R drho = f0, jx = R(0), jy = R(0), jz = R(0);
+    R v[L::Q];
 #pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        const R fi = Storage<ST>::load(f + natural_slot<L>(i, layout) * qs + nd);
-        drho += fi;
-        if (L::cx(i) > 0) jx += fi;
-        if (L::cx(i) < 0) jx -= fi;
-        if (L::cy(i) > 0) jy += fi;
-        if (L::cy(i) < 0) jy -= fi;
-        if (L::cz(i) > 0) jz += fi;
-        if (L::cz(i) < 0) jz -= fi;
-    }
+    for (int i = 0; i < L::Q; ++i) v[i] = Storage<ST>::load(f + natural_slot<L>(i, layout) * qs + nd);
     R F[3] = {R(p.force[0]), R(p.force[1]), R(p.force[2])};
     if (p.force_field != nullptr) {
         const R* ff = (const R*)p.force_field;
@@ -196,11 +186,7 @@ __global__ void macro_kernel(const lbm_grid_t g, const lbm_physics_t p, const ui
     if (list != nullptr && local != nullptr) {
         for (int a = 0; a < L::D; ++a) F[a] += local[(int64_t)a * n_list + t];
     }
-    const R rho = R(1) + drho;
-    rho_out[nd] = rho;
-    u_out[nd] = (jx - R(0.5) * F[0]) / rho;
-    u_out[qs + nd] = (jy - R(0.5) * F[1]) / rho;
-    if (L::D == 3) u_out[2 * qs + nd] = (jz - R(0.5) * F[2]) / rho;
+    store_macro<L, R>(v, F[0], F[1], F[2], nd, qs, rho_out, u_out);
 }
 
 template <class L, int ST>

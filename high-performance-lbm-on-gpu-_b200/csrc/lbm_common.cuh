@@ -749,6 +749,8 @@ struct StepArgs {
     int64_t* health_words;    // [0] first bad pitched node (atomicMin), [1] 1 if non-finite (atomicMax)
     double* health_partial;   // one float64 sum per block of the launch
     int64_t health_slot0;     // partial slot of this launch's first block
+    void* readout_rho;        // checked step: rho and u of the nodes it updates (lbm_health_t.rho / .u)
+    void* readout_u;
     lbm_special_t sp;
     bool guo_const;    // rf/rd hold kC, kG of the uniform force (else computed per node)
     Relax<float> rf;   // collision constants (float arithmetic)
@@ -791,6 +793,40 @@ __device__ __forceinline__ void health_node(NodeHealth& hl, int64_t nd, const R 
     const bool nf = !isfinite(drho);
     if (nf || drho <= R(-1)) hl.bad = nd < hl.bad ? nd : hl.bad;
     hl.nonfinite |= nf;
+}
+
+// rho and u of a node's post-collision populations v (shifted, direction
+// order) with the force F the collision applied (reference
+// macroscopic_from_post_collision, src/lbm/diagnostics.py:72-80):
+// rho = 1 + sum v, u = (sum c v - F/2) / rho, each operation rounded once.
+// The readout kernel and the readout fused into a checked step both call it,
+// so they give the same bits.
+template <class L, class R>
+__device__ __forceinline__ void macro_node(const R (&v)[L::Q], R Fx, R Fy, R Fz, R& rho, R (&u)[3])
+{
+    R drho = v[0], jx = R(0), jy = R(0), jz = R(0);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        drho = v_add(drho, v[i]);
+        if (L::cx(i)) jx = L::cx(i) > 0 ? v_add(jx, v[i]) : v_sub(jx, v[i]);
+        if (L::cy(i)) jy = L::cy(i) > 0 ? v_add(jy, v[i]) : v_sub(jy, v[i]);
+        if (L::D == 3 && L::cz(i)) jz = L::cz(i) > 0 ? v_add(jz, v[i]) : v_sub(jz, v[i]);
+    }
+    rho = v_add(R(1), drho);
+    u[0] = v_div(v_sub(jx, v_mul(R(0.5), Fx)), rho);
+    u[1] = v_div(v_sub(jy, v_mul(R(0.5), Fy)), rho);
+    u[2] = L::D == 3 ? v_div(v_sub(jz, v_mul(R(0.5), Fz)), rho) : R(0);
+}
+
+template <class L, class R>
+__device__ __forceinline__ void store_macro(const R (&v)[L::Q], R Fx, R Fy, R Fz, int64_t nd, int64_t qstride,
+                                            R* __restrict__ rho_out, R* __restrict__ u_out)
+{
+    R rho, u[3];
+    macro_node<L, R>(v, Fx, Fy, Fz, rho, u);
+    rho_out[nd] = rho;
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) u_out[a * qstride + nd] = u[a];
 }
 
 // Every thread of the block calls it once (blocks are whole warps).

@@ -165,15 +165,18 @@ struct StepKernel {
 
     // Health epilogue of a checked step (pull and AA even: the node's stored
     // values are its post-collision populations): the values as stored,
-    // rounded like the stores for 16-bit formats.
-    __device__ static __forceinline__ void stored_health(const R (&f)[Q], uint32_t h, bool hi, int64_t nd,
-                                                         NodeHealth& hl)
+    // rounded like the stores for 16-bit formats; with a readout, also the
+    // node's rho and u from them and the force its collision applied.
+    __device__ static __forceinline__ void stored_health(const StepArgs& a, const R (&f)[Q], uint32_t h, bool hi,
+                                                         int64_t nd, R Fx, R Fy, R Fz, NodeHealth& hl)
     {
         static_assert(VAR != LBM_AA_ODD, "the odd AA half does not store a node's populations at the node");
         R v[Q];
 #pragma unroll
         for (int i = 0; i < Q; ++i) v[i] = S::STOCHASTIC ? S::round_sr(f[i], h, i, hi) : f[i];
         health_node<L, R>(hl, nd, v);
+        if (a.readout_rho != nullptr)
+            store_macro<L, R>(v, Fx, Fy, Fz, nd, a.qstride, static_cast<R*>(a.readout_rho), static_cast<R*>(a.readout_u));
     }
 
     // Interior fluid node (kind 0: no solid neighbour, not on a face of the
@@ -209,7 +212,7 @@ struct StepKernel {
         }
         collide_model<L, R, CM>(f, a.template relax<R>(), a.guo_const && a.force_field == nullptr, Fx, Fy, Fz);
         const uint32_t h = S::STOCHASTIC ? sr_pair_hash(pair, a.seed[a.parity]) : 0u;
-        if constexpr (H) stored_health(f, h, hi, nd, *hl);
+        if constexpr (H) stored_health(a, f, h, hi, nd, Fx, Fy, Fz, *hl);
         T* fd = static_cast<T*>(a.f_dst) + nd;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -310,7 +313,7 @@ struct StepKernel {
         collide_model<L, R, CM>(f, a.template relax<R>(), uniform, Fx, Fy, Fz);
         const uint32_t h = S::STOCHASTIC ? sr_pair_hash(sr_pair(a.nx, a.ny, x, y, z), a.seed[a.parity]) : 0u;
         const bool hi = x & 1;
-        if constexpr (H) stored_health(f, h, hi, nd, *hl);
+        if constexpr (H) stored_health(a, f, h, hi, nd, Fx, Fy, Fz, *hl);
 
         // ---- store (16-bit formats: stochastic rounding, see sr_pair_hash)
         T* fd = static_cast<T*>(a.f_dst);

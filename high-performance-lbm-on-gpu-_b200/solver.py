@@ -296,6 +296,10 @@ class CudaSolver(Solver):
         """Total mass (sum of rho over fluid nodes, float64, summed on the device) of the state
         after the last check of the run loop; None before the first."""
         self._health_fresh = False
+        # rho and u written by the checked step of the run loop once macroscopic() has been asked
+        # for (allocated then); fresh while no other step or state change followed that step
+        self._readout = None
+        self._readout_fresh = False
 
         # ---- immersed boundary and link rules -> special nodes
         self._ibm = None
@@ -524,6 +528,8 @@ class CudaSolver(Solver):
             raise N.NativeError(f"lbm_health_partials: invalid arguments (status {n})")
         self._health_partial = torch.empty(int(n), dtype=torch.float64, device=self.device)
         self._health_struct = N.Health(N.ptr(self._health), N.ptr(self._health_partial), int(n))
+        if getattr(self, "_readout", None) is not None:
+            self._health_struct.rho, self._health_struct.u = N.ptr(self._readout[0]), N.ptr(self._readout[1:])
         bx, by = self.block
         self._checked_launches = {m: N.Launch(bx, by, m, 0, N.C.pointer(self._health_struct))
                                   for m in N.LAUNCH_MODES}
@@ -653,6 +659,7 @@ class CudaSolver(Solver):
         # starts with no report of an earlier step
         self._seed[:3].zero_()
         self._health_fresh = False
+        self._readout_fresh = False
         s = self._special
         if self.variant == "aa" and s.n_export:
             self._export_cur = s.tensors["export_a"]
@@ -796,7 +803,9 @@ class CudaSolver(Solver):
     def _advance_checked(self, steps: int) -> None:
         """``_advance``, with the state check fused into the last step (the even half of the
         last AA pair): its kernels also flag bad nodes and sum f~* in float64, and
-        ``_check_health`` reads the three words instead of scanning the lattice again."""
+        ``_check_health`` reads the three words instead of scanning the lattice again. Once
+        ``macroscopic()`` has been called, the same step also writes rho and u of the state it
+        leaves, which the next ``macroscopic()`` returns without reading the lattice again."""
         if steps <= 0:
             return
         m = self.step_multiple
@@ -811,11 +820,13 @@ class CudaSolver(Solver):
         mass_bits = self._words[4:5]  # float64 written through its int64 storage
         self._native("lbm_health_finish", N.C.byref(self._health_struct), N.ptr(mass_bits), stream)
         self._health_fresh = True
+        self._readout_fresh = self._readout is not None
 
     def _advance(self, steps: int) -> None:
         if steps <= 0:
             return
         self._health_fresh = False
+        self._readout_fresh = False
         if not self.use_graph or steps < self.GRAPH_CHUNK:
             self._launch_steps(steps)
             return
@@ -879,19 +890,33 @@ class CudaSolver(Solver):
         raise SimulationDiverged(self.time_step, location, reason)
 
     def macroscopic(self) -> MacroscopicFields:
-        """rho and u on the host (reference ``solver.py:209-221``)."""
+        """rho and u on the host (reference ``solver.py:209-221``).
+
+        Straight after the run loop's checked step (``run``), the fields that step wrote (the
+        readout fused into it, the same bits as the readout kernel); otherwise one pass of the
+        readout kernel over the lattice. The first call also asks the checked steps that follow
+        to write the fields."""
         torch = self.torch
         d = self.lattice.d
-        fields = torch.empty((d + 1, self.qstride), dtype=self.t_real, device=self.device)
-        rho, u = fields[0], fields[1:]
-        local_nodes = local = None
-        n_local = 0
-        if self._ibm is not None:
-            local_nodes = self._ibm.node
-            local = self._ibm.final_force
-            n_local = self._ibm.tables.n_nodes
-        self._native("lbm_macroscopic", N.C.byref(self.grid), N.C.byref(self.physics), N.ptr(self._kind), N.ptr(self._f),
-                     self._layout_code, N.ptr(local_nodes), N.ptr(local), n_local, N.ptr(rho), N.ptr(u), self._stream())
+        if self._readout_fresh:
+            fields = self._readout
+        else:
+            fields = torch.empty((d + 1, self.qstride), dtype=self.t_real, device=self.device)
+            rho, u = fields[0], fields[1:]
+            local_nodes = local = None
+            n_local = 0
+            if self._ibm is not None:
+                local_nodes = self._ibm.node
+                local = self._ibm.final_force
+                n_local = self._ibm.tables.n_nodes
+            self._native("lbm_macroscopic", N.C.byref(self.grid), N.C.byref(self.physics), N.ptr(self._kind),
+                         N.ptr(self._f), self._layout_code, N.ptr(local_nodes), N.ptr(local), n_local, N.ptr(rho),
+                         N.ptr(u), self._stream())
+        if self._readout is None:
+            # solid nodes keep rho = 1, u = 0: the steps write fluid nodes only
+            self._readout = torch.zeros((d + 1, self.qstride), dtype=self.t_real, device=self.device)
+            self._readout[0].fill_(1.0)
+            self._health_struct.rho, self._health_struct.u = N.ptr(self._readout[0]), N.ptr(self._readout[1:])
         host = self._from_pitched(fields)  # one copy for rho and u
         return MacroscopicFields(rho=host[0], u=tuple(host[1 + a] for a in range(d)), solid=np.array(self._solid_host))
 

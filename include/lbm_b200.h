@@ -165,6 +165,12 @@ typedef struct lbm_health {
                             node is non-finite; set both with lbm_health_reset before the step */
     double* partial;     /* n_partial doubles, written by the step (one per block) */
     int64_t n_partial;   /* exactly lbm_health_partials(grid, sp, launch) for the step's launch mode */
+    void* rho;           /* NULL, or the macroscopic readout fused into the same step (reference
+                            macroscopic_from_post_collision, src/lbm/diagnostics.py:72-80): rho (qstride)
+                            and u (d, qstride) in the compute type, pitched, of every fluid node the
+                            step updates, from the values it stores -- the bits lbm_macroscopic gives
+                            for that state; solid nodes are left as they are (fill rho = 1, u = 0) */
+    void* u;
 } lbm_health_t;
 
 typedef struct lbm_launch {

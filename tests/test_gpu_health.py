@@ -114,3 +114,55 @@ def test_closed_box_mass_stays_put_through_the_run_loop(backend):
     assert len(seen) == 4
     for m in seen:
         assert m == pytest.approx(m0, rel=1e-13)
+
+
+@pytest.mark.parametrize("backend", BACKENDS)
+@pytest.mark.parametrize("name", ["duct16", "bouzidi3d", "mixed2d", "ibm2d"])
+@pytest.mark.parametrize("launch", ["split", "fused"])
+def test_readout_fused_into_the_checked_step_equals_the_readout_kernel(backend, name, launch):
+    """Once macroscopic() has been asked for, the run loop's checked step also writes rho and u
+    (reference diagnostics.py:72-80); the next macroscopic() returns them, bit for bit what the
+    separate readout pass gives for the same state, and within the parity bounds of the oracle's."""
+    p = case(name)
+    state = cases.random_state(p)
+    gpu = lbm.make_solver(p, backend=backend, launch=launch)
+    ref = OracleSolver(p)
+    gpu.initialize(*state)
+    ref.initialize(*state)
+    gpu.run(4, check_every=4)
+    ref.run(4)
+    first = gpu.macroscopic()  # the readout pass; asks the following checked steps for the fields
+    assert not gpu._readout_fresh
+    gpu.run(8, check_every=4)
+    ref.run(8)
+    assert gpu._readout_fresh
+    fused = gpu.macroscopic()
+    gpu._readout_fresh = False  # the same state through the separate readout pass
+    separate = gpu.macroscopic()
+    np.testing.assert_array_equal(fused.rho, separate.rho)
+    for a, b in zip(fused.u, separate.u, strict=True):
+        np.testing.assert_array_equal(a, b)
+    assert not np.array_equal(first.rho, fused.rho)
+    want = ref.macroscopic()
+    tol = {"float64": 1e-14, "float32": 1e-6}.get(p.dtype, 2e-4)  # 16-bit: a few storage ulps
+    np.testing.assert_allclose(fused.rho, want[0], rtol=0, atol=tol)
+    for a in range(p.d):
+        np.testing.assert_allclose(fused.u[a], want[1][a], rtol=0, atol=tol)
+
+
+def test_a_plain_step_or_a_new_state_retires_the_fused_readout():
+    p = case("mixed2d")
+    gpu = lbm.make_solver(p, backend="cuda-naive")
+    gpu.initialize(*cases.random_state(p))
+    gpu.macroscopic()
+    gpu.run(4, check_every=4)
+    assert gpu._readout_fresh
+    gpu._advance(2)
+    assert not gpu._readout_fresh
+    gpu.run(4, check_every=4)
+    assert gpu._readout_fresh
+    gpu.initialize(*cases.random_state(p, seed=1))
+    assert not gpu._readout_fresh
+    gpu.run(4, check_every=4)
+    gpu.set_populations(gpu.populations())
+    assert not gpu._readout_fresh
