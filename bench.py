@@ -183,7 +183,8 @@ def run_reference(args, rank):
     import multiprocessing
 
     n = args.n
-    workers = max(1, os.cpu_count() or 1)
+    # the cores this process may run on (at most 64 processes, to bound host memory)
+    workers = max(1, min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count() or 1))
     # size each slab so that K steps take about a minute (a larger K is cut off at a 60 s budget);
     # with many processes the slabs stay thin to bound host memory
     per_node = 1.0 / 1.4e6
