@@ -731,6 +731,22 @@ __global__ void __launch_bounds__(256, bulk_min_blocks<ST, VAR, H || CM != LBM_C
     }
 }
 
+// D2Q9 float32 pull on planes far beyond L2 (at least WIDE_PLANE_NODES
+// nodes): a D2Q9 node has only nine loads to hide the memory latency with,
+// so a bound of eight blocks per SM (32 registers, a small spill on the
+// general path) keeps more of them in flight: 2048^2 78.2 against 74.3 GLUPS,
+// 4096^2 84.8 against 77.3. Small grids (the cylinder channel, L2-resident
+// lattices) keep the default kernel, which is faster there. Same code, so
+// the same bits.
+constexpr int64_t WIDE_PLANE_NODES = int64_t(1) << 21;
+
+template <class L, int ST>
+__global__ void __launch_bounds__(256, 8) lbm_bulk_wide_kernel(const StepArgs a)
+{
+    advance_seed(a);
+    bulk_tile<L, ST, LBM_PULL, false, LBM_COLLIDE_TRT>(a, blockIdx.z);
+}
+
 // FUSED: grid (ceil(nx/bx), ceil(ny/by), nz + extra), planes z >= nz are
 // boundary warps. BOUNDARY: 1D grid over the list. Up to 255 registers, so
 // the general per-node path never spills.
@@ -832,6 +848,12 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
             if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
                 const unsigned gxv = (unsigned)((a.nx + 2 * tile_x - 1) / (2 * tile_x));
                 lbm_bulk_vec_aa_kernel<L, ST, VAR><<<dim3(gxv, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
+                return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+            }
+        }
+        if constexpr (L::D == 2 && ST == LBM_F32 && VAR == LBM_PULL && CM == LBM_COLLIDE_TRT) {
+            if ((int64_t)a.nx * a.ny >= WIDE_PLANE_NODES) {
+                lbm_bulk_wide_kernel<L, ST><<<dim3(gx, gy, a.nz), dim3(tile_x, tile_y), 0, stream>>>(a);
                 return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
             }
         }

@@ -46,6 +46,25 @@ def test_taylor_green_512_matches_oracle_and_decays_at_the_lattice_viscosity():
 
 
 # ---------------------------------------------------------------- D3Q19 duct 256^3
+def test_large_d2q9_plane_matches_the_oracle():
+    """A D2Q9 float32 plane of 2^21 nodes (2048 x 1024, channel walls, a body force) takes the
+    register-bounded pull kernel for large planes; it must give the oracle's step like every other."""
+    nx, ny = 2048, 1024
+    solid = np.zeros((ny, nx), dtype=bool)
+    solid[[0, -1], :] = True
+    p = NS.SimulationParams(nx=nx, ny=ny, tau=0.6, collision="trt", solid=solid, force=(1e-5, -2e-6),
+                            dtype="float32")
+    state = cases.random_state(p)
+    ref = OracleSolver(p)
+    gpu = lbm.make_solver(p, backend="cuda-naive")
+    ref.initialize(*state)
+    gpu.initialize(*state)
+    ref.run(3)
+    gpu.run(3)
+    a, b = ref.populations()[:, p.fluid], gpu.populations()[:, p.fluid]
+    assert np.abs(a - b).max() < 1e-7
+
+
 @pytest.mark.parametrize("storage", ["float32", "float16", "bfloat16"])
 def test_duct_256_pull_and_aa_agree_bit_for_bit(storage):
     p = cases.duct(NS, n=256, dtype=storage)
