@@ -678,6 +678,93 @@ __global__ void __launch_bounds__(256, odd_rows_min_blocks<ST, CM>()) lbm_aa_odd
     }
 }
 
+// ---------------------------------------------------------------- odd AA, rows, 16-bit
+// The odd AA half for 16-bit storage with one block per row (nx even, at
+// most 256: 128 threads), each thread a node pair (x0, x0 + 1): a row whose nodes are all
+// interior in y and z (kinds 0 and EDGE, the row off the y and z faces) reads
+// each direction's source pair words from row (y - c_y, z - c_z) of slot
+// opp(i) -- the pair's own word, and the neighbouring pair's word for
+// directions with c_x != 0 (x wrapped in the row) -- collides the pair as the
+// other pair kernels do, rounds it, writes its results into shared memory in
+// destination order (x + c_x, wrapped) and, after one barrier, stores every
+// destination row (y + c_y, z + c_z) of slot i as aligned pair words. Other
+// rows run the one-node path. Same bits as every other kernel of the step;
+// in place is safe as in the 4- and 8-byte row kernel: slot i of row
+// (y + c_y, z + c_z) is read in this half only by the nodes of row (y, z).
+template <class L, int ST>
+__global__ void __launch_bounds__(128, 6) lbm_aa_odd_pair_rows_kernel(const StepArgs a)
+{
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    constexpr int Q = L::Q;
+    static_assert(sizeof(T) == 2, "two 16-bit populations per word");
+    extern __shared__ __align__(16) unsigned char pair_rows_smem[];
+    unsigned short* out = reinterpret_cast<unsigned short*>(pair_rows_smem);  // [Q][nx]
+    advance_seed(a);
+    const int nx = a.nx, y = blockIdx.x, z = blockIdx.y;
+    const int x0 = 2 * threadIdx.x;
+    const bool in = x0 < nx;
+    const int64_t py = a.pitch, pz = (int64_t)a.pitch * a.ny, qs = a.qstride;
+    const int64_t row = (int64_t)z * pz + (int64_t)y * py;
+    const int64_t nd0 = row + x0;
+    const uint32_t k2 = in ? *reinterpret_cast<const unsigned short*>(a.kind + nd0) : 0u;
+    const bool row_ok = y >= 1 && y <= a.ny - 2 && (L::D == 2 || (z >= 1 && z <= a.nz - 2));
+    if (!__syncthreads_and(row_ok && (k2 & ~0x0808u) == 0u)) {
+        for (int h = 0; h < 2; ++h) bulk_node<L, ST, LBM_AA_ODD>(a, x0 + h, y, z, nd0 + h, in);
+        return;
+    }
+    if (in) {
+        const int wm = (x0 == 0 ? nx - 2 : x0 - 2) >> 1;  // the previous pair's word, wrapped
+        const int wo = x0 >> 1;
+        const int wn = (x0 + 2 == nx ? 0 : x0 + 2) >> 1;  // the next pair's word, wrapped
+        const unsigned short* fs = static_cast<const unsigned short*>(a.f_src);
+        R fa[Q], fb[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(
+                fs + (L::opp(i) * qs + row - (L::cy(i) * py + L::cz(i) * pz)));
+            if (L::cx(i) == 0) {
+                const uint32_t v = w[wo];
+                fa[i] = S::decode_lo(v);
+                fb[i] = S::decode_hi(v);
+            } else if (L::cx(i) > 0) {  // sources x0 - 1, x0
+                fa[i] = S::decode_hi(w[wm]);
+                fb[i] = S::decode_lo(w[wo]);
+            } else {  // sources x0 + 1, x0 + 2
+                fa[i] = S::decode_hi(w[wo]);
+                fb[i] = S::decode_lo(w[wn]);
+            }
+        }
+        collide_pair<L, S::SCALE_LOG2>(fa, fb, a.template relax<R>(), R(a.fx), R(a.fy), R(a.fz));
+        const uint32_t h = sr_pair_hash(sr_pair(nx, a.ny, x0, y, z), a.seed[a.parity]);
+        const int xm = x0 == 0 ? nx - 1 : x0 - 1;
+        const int xp = x0 + 2 == nx ? 0 : x0 + 2;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const uint32_t v = S::pack_sr(fa[i], fb[i], sr_word(h, i));  // (x0, x0 + 1) rounded
+            unsigned short* o = out + i * nx;
+            if (L::cx(i) == 0) {
+                *reinterpret_cast<uint32_t*>(o + x0) = v;
+            } else if (L::cx(i) > 0) {  // x0 -> x0 + 1, x0 + 1 -> x0 + 2
+                o[x0 + 1] = (unsigned short)v;
+                o[xp] = (unsigned short)(v >> 16);
+            } else {  // x0 -> x0 - 1, x0 + 1 -> x0
+                o[xm] = (unsigned short)v;
+                o[x0] = (unsigned short)(v >> 16);
+            }
+        }
+    }
+    __syncthreads();
+    if (in) {
+        T* f = static_cast<T*>(a.f_dst);
+#pragma unroll
+        for (int i = 0; i < Q; ++i)
+            *reinterpret_cast<uint32_t*>(f + (i * qs + row + (L::cy(i) * py + L::cz(i) * pz) + x0)) =
+                *reinterpret_cast<const uint32_t*>(out + i * nx + x0);
+    }
+}
+
 // Storage formats with the pair and TMA kernels (float32 and float64 keep
 // the one-node kernel: it is faster there).
 template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_BF16; }
@@ -844,6 +931,19 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
         if constexpr (VAR != LBM_PULL && has_vec<ST>() && CM == LBM_COLLIDE_TRT) {
             int status = LBM_OK;
             if (launch_tma<L, ST, VAR>(a, stream, &status)) return status;
+            // the odd half on widths the TMA kernel does not take: one block per row (same speed
+            // as the TMA kernel where both apply)
+            if constexpr (VAR == LBM_AA_ODD) {
+                if (a.nx % 2 == 0 && a.nx <= 2 * 128 && a.ny <= 65535 && a.pitch % 2 == 0 && a.qstride % 2 == 0 &&
+                    a.force_field == nullptr && a.guo_const && a.seed != nullptr &&
+                    reinterpret_cast<uintptr_t>(a.kind) % 2 == 0 && reinterpret_cast<uintptr_t>(a.f_src) % 4 == 0 &&
+                    reinterpret_cast<uintptr_t>(a.f_dst) % 4 == 0) {
+                    const unsigned threads = (unsigned)((a.nx / 2 + 31) / 32 * 32);
+                    const size_t smem = (size_t)L::Q * a.nx * sizeof(typename Storage<ST>::T);
+                    lbm_aa_odd_pair_rows_kernel<L, ST><<<dim3((unsigned)a.ny, (unsigned)a.nz), threads, smem, stream>>>(a);
+                    return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+                }
+            }
             // node pairs: every row and direction plane starts on an even node
             if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
                 const unsigned gxv = (unsigned)((a.nx + 2 * tile_x - 1) / (2 * tile_x));
