@@ -765,6 +765,64 @@ __global__ void __launch_bounds__(128, 6) lbm_aa_odd_pair_rows_kernel(const Step
     }
 }
 
+// The two-lattice pull for 16-bit storage on widths the TMA kernel does not
+// take, one block per row (nx even, at most 256), each thread a node pair:
+// a row whose nodes are all interior in y and z (kinds 0 and EDGE, the row off
+// the y and z faces) reads each direction's source pair words from row
+// (y - c_y, z - c_z) of slot i -- the pair's own word, and the neighbouring
+// pair's word for directions with c_x != 0 (x wrapped in the row) -- collides
+// the pair as the other pair kernels do and stores aligned pair words. No
+// warp straddles two rows, so no row falls back for that; rows with other
+// nodes run the one-node path. Same bits as every other kernel of the step.
+template <class L, int ST>
+__global__ void __launch_bounds__(128, 6) lbm_pull_pair_rows_kernel(const StepArgs a)
+{
+    using S = Storage<ST>;
+    using T = typename S::T;
+    using R = typename S::R;
+    constexpr int Q = L::Q;
+    static_assert(sizeof(T) == 2, "two 16-bit populations per word");
+    advance_seed(a);
+    const int nx = a.nx, y = blockIdx.x, z = blockIdx.y;
+    const int x0 = 2 * threadIdx.x;
+    const bool in = x0 < nx;
+    const int64_t py = a.pitch, pz = (int64_t)a.pitch * a.ny, qs = a.qstride;
+    const int64_t row = (int64_t)z * pz + (int64_t)y * py;
+    const int64_t nd0 = row + x0;
+    const uint32_t k2 = in ? *reinterpret_cast<const unsigned short*>(a.kind + nd0) : 0u;
+    const bool row_ok = y >= 1 && y <= a.ny - 2 && (L::D == 2 || (z >= 1 && z <= a.nz - 2));
+    if (!__syncthreads_and(row_ok && (k2 & ~0x0808u) == 0u)) {
+        for (int h = 0; h < 2; ++h) bulk_node<L, ST, LBM_PULL>(a, x0 + h, y, z, nd0 + h, in);
+        return;
+    }
+    if (!in) return;
+    const int wm = (x0 == 0 ? nx - 2 : x0 - 2) >> 1;  // the previous pair's word, wrapped
+    const int wo = x0 >> 1;
+    const int wn = (x0 + 2 == nx ? 0 : x0 + 2) >> 1;  // the next pair's word, wrapped
+    const unsigned short* fs = static_cast<const unsigned short*>(a.f_src);
+    R fa[Q], fb[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(fs + (i * qs + row - (L::cy(i) * py + L::cz(i) * pz)));
+        if (L::cx(i) == 0) {
+            const uint32_t v = __ldg(w + wo);
+            fa[i] = S::decode_lo(v);
+            fb[i] = S::decode_hi(v);
+        } else if (L::cx(i) > 0) {  // sources x0 - 1, x0
+            fa[i] = S::decode_hi(__ldg(w + wm));
+            fb[i] = S::decode_lo(__ldg(w + wo));
+        } else {  // sources x0 + 1, x0 + 2
+            fa[i] = S::decode_hi(__ldg(w + wo));
+            fb[i] = S::decode_lo(__ldg(w + wn));
+        }
+    }
+    collide_pair<L, S::SCALE_LOG2>(fa, fb, a.template relax<R>(), R(a.fx), R(a.fy), R(a.fz));
+    const uint32_t h = sr_pair_hash(sr_pair(nx, a.ny, x0, y, z), a.seed[a.parity]);
+    T* fd = static_cast<T*>(a.f_dst) + nd0;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) *reinterpret_cast<uint32_t*>(fd + i * qs) = S::pack_sr(fa[i], fb[i], sr_word(h, i));
+}
+
 // Storage formats with the pair and TMA kernels (float32 and float64 keep
 // the one-node kernel: it is faster there).
 template <int ST> constexpr bool has_vec() { return ST == LBM_F16 || ST == LBM_BF16; }
@@ -912,6 +970,15 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
         if constexpr (VAR == LBM_PULL && has_vec<ST>() && CM == LBM_COLLIDE_TRT) {
             int status = LBM_OK;
             if (launch_tma<L, ST, LBM_PULL>(a, stream, &status)) return status;
+            // widths the TMA kernel does not take: one block per row
+            if (a.nx % 2 == 0 && a.nx <= 2 * 128 && a.ny <= 65535 && a.pitch % 2 == 0 && a.qstride % 2 == 0 &&
+                a.force_field == nullptr && a.guo_const && a.seed != nullptr &&
+                reinterpret_cast<uintptr_t>(a.kind) % 2 == 0 && reinterpret_cast<uintptr_t>(a.f_src) % 4 == 0 &&
+                reinterpret_cast<uintptr_t>(a.f_dst) % 4 == 0) {
+                const unsigned threads = (unsigned)((a.nx / 2 + 31) / 32 * 32);
+                lbm_pull_pair_rows_kernel<L, ST><<<dim3((unsigned)a.ny, (unsigned)a.nz), threads, 0, stream>>>(a);
+                return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+            }
             // pairs need every row and direction plane to start on an even
             // node, and the launch's uniform-force constants
             if (a.pitch % 2 == 0 && a.qstride % 2 == 0 && a.force_field == nullptr && a.guo_const) {
