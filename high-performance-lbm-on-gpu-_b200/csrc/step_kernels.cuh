@@ -765,17 +765,20 @@ __global__ void __launch_bounds__(128, 6) lbm_aa_odd_pair_rows_kernel(const Step
     }
 }
 
-// The two-lattice pull for 16-bit storage on widths the TMA kernel does not
-// take, one block per row (nx even, at most 256), each thread a node pair:
-// a row whose nodes are all interior in y and z (kinds 0 and EDGE, the row off
-// the y and z faces) reads each direction's source pair words from row
-// (y - c_y, z - c_z) of slot i -- the pair's own word, and the neighbouring
-// pair's word for directions with c_x != 0 (x wrapped in the row) -- collides
-// the pair as the other pair kernels do and stores aligned pair words. No
-// warp straddles two rows, so no row falls back for that; rows with other
-// nodes run the one-node path. Same bits as every other kernel of the step.
-template <class L, int ST>
-__global__ void __launch_bounds__(128, 6) lbm_pull_pair_rows_kernel(const StepArgs a)
+// The two-lattice pull (VAR = LBM_PULL) and the even AA half (LBM_AA_EVEN)
+// for 16-bit storage on widths the TMA kernel does not take, one block per
+// row (nx even, at most 256), each thread a node pair: a row whose nodes are
+// all interior in y and z (kinds 0 and EDGE, the row off the y and z faces)
+// reads each direction's pair words -- pull: from row (y - c_y, z - c_z) of
+// slot i, the pair's own word and, for directions with c_x != 0, the
+// neighbouring pair's word (x wrapped in the row); even AA half: the pair's
+// own word of slot i -- collides the pair as the other pair kernels do and
+// stores aligned pair words (pull: slot i; even AA half: slot opp(i), in
+// place, node-local). No warp straddles two rows, so no row falls back for
+// that; rows with other nodes run the one-node path. Same bits as every other
+// kernel of the step.
+template <class L, int ST, int VAR>
+__global__ void __launch_bounds__(128, 6) lbm_pair_rows_kernel(const StepArgs a)
 {
     using S = Storage<ST>;
     using T = typename S::T;
@@ -792,7 +795,7 @@ __global__ void __launch_bounds__(128, 6) lbm_pull_pair_rows_kernel(const StepAr
     const uint32_t k2 = in ? *reinterpret_cast<const unsigned short*>(a.kind + nd0) : 0u;
     const bool row_ok = y >= 1 && y <= a.ny - 2 && (L::D == 2 || (z >= 1 && z <= a.nz - 2));
     if (!__syncthreads_and(row_ok && (k2 & ~0x0808u) == 0u)) {
-        for (int h = 0; h < 2; ++h) bulk_node<L, ST, LBM_PULL>(a, x0 + h, y, z, nd0 + h, in);
+        for (int h = 0; h < 2; ++h) bulk_node<L, ST, VAR>(a, x0 + h, y, z, nd0 + h, in);
         return;
     }
     if (!in) return;
@@ -803,6 +806,12 @@ __global__ void __launch_bounds__(128, 6) lbm_pull_pair_rows_kernel(const StepAr
     R fa[Q], fb[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
+        if constexpr (VAR == LBM_AA_EVEN) {  // node-local, in place: plain loads
+            const uint32_t v = *reinterpret_cast<const uint32_t*>(fs + (i * qs + nd0));
+            fa[i] = S::decode_lo(v);
+            fb[i] = S::decode_hi(v);
+            continue;
+        }
         const uint32_t* w = reinterpret_cast<const uint32_t*>(fs + (i * qs + row - (L::cy(i) * py + L::cz(i) * pz)));
         if (L::cx(i) == 0) {
             const uint32_t v = __ldg(w + wo);
@@ -820,7 +829,9 @@ __global__ void __launch_bounds__(128, 6) lbm_pull_pair_rows_kernel(const StepAr
     const uint32_t h = sr_pair_hash(sr_pair(nx, a.ny, x0, y, z), a.seed[a.parity]);
     T* fd = static_cast<T*>(a.f_dst) + nd0;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) *reinterpret_cast<uint32_t*>(fd + i * qs) = S::pack_sr(fa[i], fb[i], sr_word(h, i));
+    for (int i = 0; i < Q; ++i)
+        *reinterpret_cast<uint32_t*>(fd + (VAR == LBM_AA_EVEN ? L::opp(i) : i) * qs) =
+            S::pack_sr(fa[i], fb[i], sr_word(h, i));
 }
 
 // Storage formats with the pair and TMA kernels (float32 and float64 keep
@@ -976,7 +987,7 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
                 reinterpret_cast<uintptr_t>(a.kind) % 2 == 0 && reinterpret_cast<uintptr_t>(a.f_src) % 4 == 0 &&
                 reinterpret_cast<uintptr_t>(a.f_dst) % 4 == 0) {
                 const unsigned threads = (unsigned)((a.nx / 2 + 31) / 32 * 32);
-                lbm_pull_pair_rows_kernel<L, ST><<<dim3((unsigned)a.ny, (unsigned)a.nz), threads, 0, stream>>>(a);
+                lbm_pair_rows_kernel<L, ST, LBM_PULL><<<dim3((unsigned)a.ny, (unsigned)a.nz), threads, 0, stream>>>(a);
                 return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
             }
             // pairs need every row and direction plane to start on an even
@@ -999,7 +1010,17 @@ static int launch_mode(const StepArgs& a, int mode, int tile_x, int tile_y, cuda
             int status = LBM_OK;
             if (launch_tma<L, ST, VAR>(a, stream, &status)) return status;
             // the odd half on widths the TMA kernel does not take: one block per row (same speed
-            // as the TMA kernel where both apply)
+            // as the TMA kernel where both apply); the even half likewise
+            if constexpr (VAR == LBM_AA_EVEN) {
+                if (a.nx % 2 == 0 && a.nx <= 2 * 128 && a.ny <= 65535 && a.pitch % 2 == 0 && a.qstride % 2 == 0 &&
+                    a.force_field == nullptr && a.guo_const && a.seed != nullptr &&
+                    reinterpret_cast<uintptr_t>(a.kind) % 2 == 0 && reinterpret_cast<uintptr_t>(a.f_src) % 4 == 0 &&
+                    reinterpret_cast<uintptr_t>(a.f_dst) % 4 == 0) {
+                    const unsigned threads = (unsigned)((a.nx / 2 + 31) / 32 * 32);
+                    lbm_pair_rows_kernel<L, ST, LBM_AA_EVEN><<<dim3((unsigned)a.ny, (unsigned)a.nz), threads, 0, stream>>>(a);
+                    return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_LAUNCH;
+                }
+            }
             if constexpr (VAR == LBM_AA_ODD) {
                 if (a.nx % 2 == 0 && a.nx <= 2 * 128 && a.ny <= 65535 && a.pitch % 2 == 0 && a.qstride % 2 == 0 &&
                     a.force_field == nullptr && a.guo_const && a.seed != nullptr &&
