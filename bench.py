@@ -660,7 +660,7 @@ def setup_study(lbm, torch):
 
 def kernels_study(lbm, torch):
     """Every kernel family outside the headline step, each launched a few times on a small case
-    whose inputs exceed L2 (a few hundred MB on the device), timed with CUDA events: the driver of
+    whose inputs exceed L2 (a few hundred MB on the device), timed with CUDA events: the workload of
     the per-family ncu launch list (``ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,
     dram__bytes_write.sum``). Families: the 16-bit node-pair fallbacks (nx = 200, pull and AA);
     on a 192^3 float32 duct the checked step (state check fused), the separate scan, the
