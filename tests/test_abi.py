@@ -127,3 +127,17 @@ def test_zou_he_builder_rejects_invalid_arguments_without_a_gpu(change):
     common = (ctypes.byref(grid), a["solid"], a["column"], a["sign"], a["layer_x"], a["layer"], a["velocity"], 1.0)
     assert lib.lbm_zou_he_count(*common, a["scratch"], None) == N.LBM_ERR_INVALID
     assert lib.lbm_zou_he_write(*common, a["scratch"], 14, one, one, one, one, one, one, None) == N.LBM_ERR_INVALID
+
+
+@pytest.mark.parametrize("storage,nx,pitch", [
+    ("float32", 256, 256), ("float32", 250, 256), ("float32", 2050, 2080), ("float32", 880, 896),
+    ("float32", 40, 40),  # 64 columns would add more than a quarter
+    ("float64", 40, 48), ("float64", 30, 32), ("float64", 250, 256), ("float64", 12, 12),
+    ("float16", 200, 208), ("bfloat16", 250, 256), ("float16", 10, 16),
+])
+def test_default_row_pitch(storage, nx, pitch):
+    """4- and 8-byte rows start on 128-byte boundaries when that adds at most a quarter to the row;
+    16-bit rows are padded to 16 nodes (the pair and TMA kernels' 16-byte row strides)."""
+    from lbm_b200.solver import row_pitch
+
+    assert row_pitch(nx, storage) == pitch
