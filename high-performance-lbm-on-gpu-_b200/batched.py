@@ -82,8 +82,9 @@ class BatchedSolver:
             shape = tuple(p.shape)
             nx, ny = shape[-1], shape[-2]
             nz = shape[0] if d == 3 else 1
-            # unpadded rows: padding them to 128 bytes (row_pitch) made the batched step
-            # slower on the 256-cavity batch (54.7 against 60.9 GLUPS), unlike a lone lattice
+            # unpadded rows: padded ones made the batched step slower on the 256-cavity
+            # batch (32-byte rows 59.8, 128-byte rows 54.7, against 60.4-60.9 GLUPS),
+            # unlike a lone lattice (row_pitch)
             pitch = nx
             qstride = -(-pitch * ny * nz // PLANE_ALIGN) * PLANE_ALIGN
             self.grids.append(N.Grid(N.LATTICE_CODE[lat.name], N.STORAGE_CODE[dtype], nx, ny, nz, pitch, qstride))

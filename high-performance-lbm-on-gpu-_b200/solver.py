@@ -186,16 +186,17 @@ def row_pitch(nx: int, storage: str) -> int:
     """Default row stride (in nodes) of a lattice of width nx.
 
     16-bit storage: nx rounded up to 16 nodes (the pair and TMA kernels need
-    16-byte row strides). 4- and 8-byte storage: nx rounded up to 128 bytes
-    when that adds at most a quarter to the row, else nx -- rows that start on
-    a 128-byte boundary let a warp's 32 nodes fill whole cache lines (float32
-    pull, one B200: D2Q9 2050 x 2048 70.1 -> 75.4 GLUPS with pitch 2080,
-    D3Q19 250 x 256^2 34.2 -> 37.0 with pitch 256). Padding columns are never
-    read or written.
+    16-byte row strides). 4- and 8-byte storage: nx rounded up to 32 bytes
+    (a DRAM sector) when that adds at most a quarter to the row, else nx.
+    Rows that start only 8-byte aligned cost 7-8 % (float32 pull, one B200:
+    D2Q9 2050 x 2048 70.9 GLUPS at pitch 2050, 76.5 at 2056, 75.9 at 2064,
+    74.8 at 2080; D3Q19 250 x 256^2 476 -> 446 us per step at pitch 256);
+    wider alignment gains nothing more (D3Q19 244 x 256^2: 37.3, 37.0, 36.0
+    GLUPS at pitch 244, 248, 256). Padding columns are never read or written.
     """
     if storage in ("float16", "bfloat16"):
         return -(-nx // 16) * 16
-    align = 128 // (8 if storage == "float64" else 4)
+    align = 32 // (8 if storage == "float64" else 4)
     padded = -(-nx // align) * align
     return padded if 4 * padded <= 5 * nx else nx
 
