@@ -141,3 +141,33 @@ def test_default_row_pitch(storage, nx, pitch):
     from lbm_b200.solver import row_pitch
 
     assert row_pitch(nx, storage) == pitch
+
+
+@pytest.mark.parametrize("change", ["null_batch", "same_buffers", "no_domains", "no_kind", "no_nbr", "n_domains",
+                                    "n_tiles", "no_tiles", "tile_x", "tile_y", "tile_size", "blocks", "no_seed_16bit",
+                                    "lattice", "storage"])
+def test_batch_step_rejects_invalid_arguments_without_a_gpu(change):
+    """Every rejection of lbm_batch_step returns before any CUDA call (each case breaks one
+    argument of an otherwise complete batch), so it runs on a machine without a GPU."""
+    lib = N.load()
+    one = 16  # stands in for a device pointer; never dereferenced on these paths
+    fields = {"lattice": N.LBM_D2Q9, "storage": N.LBM_F32, "n_domains": 2, "domains": one, "n_tiles": 4, "tiles": one,
+              "tile_x": 32, "tile_y": 4, "blocks": 8, "kind": one, "solid_nbr": one, "wall_u": None,
+              "round_seed": None}
+    src, dst = one, 32
+    bad = {"no_domains": ("domains", None), "no_kind": ("kind", None), "no_nbr": ("solid_nbr", None),
+           "n_domains": ("n_domains", 0), "n_tiles": ("n_tiles", -1), "no_tiles": ("tiles", None),
+           "tile_x": ("tile_x", 48), "tile_y": ("tile_y", 0), "tile_size": ("tile_y", 9), "blocks": ("blocks", 0),
+           "lattice": ("lattice", 7), "storage": ("storage", 9)}
+    if change in bad:
+        key, value = bad[change]
+        fields[key] = value
+    if change == "no_seed_16bit":
+        fields["storage"] = N.LBM_F16
+    if change == "same_buffers":
+        dst = src
+    batch = N.Batch(**fields)
+    arg = None if change == "null_batch" else ctypes.byref(batch)
+    assert lib.lbm_batch_step(arg, ctypes.c_void_p(src), ctypes.c_void_p(dst), None) == N.LBM_ERR_INVALID
+    assert lib.lbm_batch_occupancy(N.LBM_D2Q9, N.LBM_F32, 32, 4, None) == N.LBM_ERR_INVALID
+    assert lib.lbm_batch_occupancy(N.LBM_D2Q9, N.LBM_F32, 0, 4, ctypes.byref(ctypes.c_int32())) == N.LBM_ERR_INVALID
