@@ -531,8 +531,7 @@ static bool make_adj(AdjArgs& A, const lbm_grid_t* g, const lbm_physics_t* p, co
                      const lbm_adjoint_t* adj, const uint8_t* kind, const void* f_t, const void* mu_next, void* mu_out,
                      double loss_scale)
 {
-    if (!g || !p || !adj || !kind || g->qstride < (int64_t)g->pitch * g->ny * g->nz || g->pitch < g->nx) return false;
-    if (g->lattice == LBM_D2Q9 && g->nz != 1) return false;
+    if (!grid_valid(g) || !p || !adj || !kind) return false;
     if (p->collision != LBM_COLLIDE_TRT) return false;  // the transposed collision is TRT/BGK's
     StepArgs& a = A.a;
     a.nx = g->nx;

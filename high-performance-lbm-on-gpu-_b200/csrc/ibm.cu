@@ -782,7 +782,7 @@ using namespace lbm;
 
 static bool ibm_ok(const lbm_grid_t* g, const lbm_ibm_t* ib)
 {
-    if (!g || !ib || ib->n_nodes < 0 || ib->n_markers < 0) return false;
+    if (!grid_valid(g) || !ib || ib->n_nodes < 0 || ib->n_markers < 0) return false;
     const int expect = g->lattice == LBM_D2Q9 ? 9 : 27;
     if (ib->n_nodes > 0 && (ib->stencil_size != expect || !ib->node || !ib->stencil || !ib->weight || !ib->area ||
                             !ib->inv_start || !ib->inv_marker || !ib->inv_weight || !ib->rho || !ib->u_star ||

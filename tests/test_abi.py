@@ -171,3 +171,33 @@ def test_batch_step_rejects_invalid_arguments_without_a_gpu(change):
     assert lib.lbm_batch_step(arg, ctypes.c_void_p(src), ctypes.c_void_p(dst), None) == N.LBM_ERR_INVALID
     assert lib.lbm_batch_occupancy(N.LBM_D2Q9, N.LBM_F32, 32, 4, None) == N.LBM_ERR_INVALID
     assert lib.lbm_batch_occupancy(N.LBM_D2Q9, N.LBM_F32, 0, 4, ctypes.byref(ctypes.c_int32())) == N.LBM_ERR_INVALID
+
+
+def _grid_entry_points():
+    names = [n for n, a in N._SIGNATURES.items() if a and a[0] is ctypes.POINTER(N.Grid)]
+    return sorted(set(names) | {"lbm_health_partials", "lbm_ball_links_scratch", "lbm_zou_he_scratch"})
+
+
+@pytest.mark.parametrize("name", _grid_entry_points())
+def test_every_grid_entry_point_rejects_an_invalid_grid_without_a_gpu(name):
+    """Each entry point that takes a grid checks it before any CUDA call: a grid with pitch < nx
+    (every other argument present, distinct stand-in pointers that are never dereferenced)
+    returns LBM_ERR_INVALID, so this runs on a machine without a GPU."""
+    lib = N.load()
+    fn = getattr(lib, name)
+    bad = N.Grid(N.LBM_D3Q19, N.LBM_F32, 12, 9, 5, 11, 12 * 9 * 5)  # pitch < nx
+    args, keep = [], []
+    for k, t in enumerate(fn.argtypes or [ctypes.POINTER(N.Grid)]):
+        if t is ctypes.POINTER(N.Grid):
+            args.append(ctypes.byref(bad))
+        elif isinstance(t, type) and issubclass(t, ctypes._Pointer) and issubclass(t._type_, ctypes.Structure):
+            s = t._type_()
+            keep.append(s)
+            args.append(ctypes.byref(s))
+        elif t is ctypes.c_void_p:
+            args.append(ctypes.c_void_p(4096 * (k + 1)))
+        elif t in (ctypes.c_double, ctypes.c_float):
+            args.append(1.0)
+        else:
+            args.append(1)
+    assert fn(*args) == N.LBM_ERR_INVALID
